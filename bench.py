@@ -1,0 +1,348 @@
+#!/usr/bin/env python3
+"""Benchmark: SSSP GTEPS with delta-stepping on RMAT-24 (uint32 weights).
+
+Workload (one GPU, the metric's configuration): RMAT scale 24, edge factor 16,
+a,b,c,d = .57,.19,.19,.05, symmetrised, self-loops and duplicates removed,
+uint32 weights U{1..255}; 16 seeded random sources with nonzero degree.  A
+step is one single-source solve by the library's persistent delta-stepping
+kernel (fixed Near-Far delta, or the learned policy with --policy learned).
+Steps cycle through the 16 sources.
+
+value  = sum over timed steps of reached edges / device time (GTEPS), inputs
+         resident in HBM (graph 4+ GB > L2, so no L2 flush is needed).
+e2e    = the same through the public C ABI with the per-step input (source id)
+         copied from pinned host memory and the whole distance array copied
+         back to pinned host memory inside the timed region.
+roofline: algorithmic bytes of one solve = 8*m_r (dst+weight of each reached
+         arc) + 8*n_r (rowptr pairs of reached vertices) + 8*n (label init and
+         final write) over the persistent kernel's CUDA-event time, against
+         the measured HBM copy bandwidth.
+cpu_baseline / --impl reference: the reference's CPU path (min-plus
+         Bellman-Ford, numpy, pytorch_testing/.../minplus_bellman_ford.py:51-102)
+         restated in oracle/pyoracle.py, timed on a bounded row sample of one
+         iteration and scaled to a full solve (iterations x rows).
+
+Multi-GPU (torchrun, --gpus N): replicas; every rank holds its own copy of
+the graph and solves its share of the sources (no collective on the data
+path); value = all ranks' reached edges / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rips2026-amd_b200"))
+
+SCALE = int(os.environ.get("B2_BENCH_SCALE", "24"))
+EDGE_FACTOR = 16
+SEED = 1
+NSRC = 16
+
+
+def load_peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic() -> float | None:
+    """dram bytes per launch of the persistent kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "sssp_delta_rmat24.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.th = None
+        self.active = False
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            if self.active:
+                self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def pick_sources(hg, k: int, seed: int) -> list[int]:
+    rng = np.random.default_rng(seed)
+    deg = np.diff(hg.rowptr)
+    out = []
+    while len(out) < k:
+        s = int(rng.integers(0, hg.n))
+        if deg[s] > 0:
+            out.append(s)
+    return out
+
+
+def cpu_reference_sample(hg, iterations: int, budget_s: float = 12.0) -> dict:
+    """Time the reference's min-plus BF iteration (numpy port) on a row sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    gi = hg  # symmetric weights: incoming CSR == outgoing CSR
+    n = gi.n
+    rows = n
+    # rows whose arcs fit ~1/16 of the graph per timing run
+    target = max(1, gi.m // 16)
+    rows = int(np.searchsorted(gi.rowptr, target))
+    rows = max(1, min(rows, n))
+    rp = gi.rowptr[: rows + 1].astype(np.int64)
+    ci = gi.colind[: rp[-1]]
+    dv = gi.weights[: rp[-1]].astype(np.float64)
+    d = np.full(n, np.inf)
+    d[0] = 0.0
+    d[np.random.default_rng(0).integers(0, n, n // 4)] = 1.0   # a partially reached label vector
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        dn = np.minimum(d[:rows], pyoracle.tropical_spmv(rp, ci, dv, d))
+        reps += 1
+        if time.perf_counter() - t0 > budget_s / 2 or reps >= 3:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    arcs = int(rp[-1])
+    per_iter = dt * gi.m / max(arcs, 1)
+    return {"seconds_per_iteration": per_iter, "iterations": iterations,
+            "sample": f"{reps}x tropical_spmv over rows [0,{rows}) = {arcs} arcs of {gi.m}, scaled to all arcs "
+                      f"and {iterations} Bellman-Ford iterations",
+            "cores": 1}
+
+
+def cpu_iterations_and_dijkstra(hg, source: int) -> tuple[int, float]:
+    """Jacobi BF round count for `source` from the oracle's (dist, hops)
+    Dijkstra, and that Dijkstra's single-core time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    t0 = time.perf_counter()
+    iters, _ = pyoracle.bf_iterations_u32(hg.rowptr, hg.colind, hg.weights, source)
+    return iters, time.perf_counter() - t0
+
+
+def reference_arm(args, hg, sources, config) -> dict:
+    """The reference's CPU Bellman-Ford (numpy port) on this workload, host cores only."""
+    iters, t_dij = cpu_iterations_and_dijkstra(hg, sources[0])
+    smp = cpu_reference_sample(hg, iters)
+    t_solve = smp["seconds_per_iteration"] * smp["iterations"]
+    deg = np.diff(hg.rowptr)
+    reached_edges = float(deg[deg > 0].sum())   # RMAT: every vertex with an edge is in the giant component
+    gteps = reached_edges / t_solve / 1e9
+    return {"metric": "sssp_gteps", "value": gteps, "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_solve * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config, "impl": "reference",
+            "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": 1, "kind": "port",
+                             "sample": smp["sample"]},
+            "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "detail": {"cpu_dijkstra_1core_seconds": t_dij, "bf_iterations": iters}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--policy", default="fixed", choices=["fixed", "learned"])
+    ap.add_argument("--method", default="delta", choices=["delta", "bf", "adds"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import torch
+    import torch.distributed as dist
+    distributed = world > 1 and args.impl == "ours"
+    if args.impl == "reference" and rank != 0:
+        return   # the reference arm is rank 0's CPU run; other ranks do no work
+    if distributed:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    import b200sssp
+    t_gen = time.time()
+    hg = b200sssp.gen_rmat(SCALE, EDGE_FACTOR, 0.57, 0.19, 0.19, 1, 255, SEED)
+    t_gen = time.time() - t_gen
+    sources = pick_sources(hg, NSRC, SEED)
+    config = {"workload": f"rmat{SCALE}_ef{EDGE_FACTOR}_sym_u32w1-255_delta_sssp", "scale": SCALE,
+              "edge_factor": EDGE_FACTOR, "n": hg.n, "m": hg.m, "sources": NSRC, "weights": "uint32 U{1..255}",
+              "method": args.method, "policy": args.policy,
+              "l2": "inputs larger than L2 (graph %.1f GB); no flush" % ((8 * hg.m + 8 * hg.n) / 1e9)}
+
+    if args.impl == "reference":
+        if rank == 0:
+            line = reference_arm(args, hg, sources, config)
+            print(json.dumps(line), flush=True)
+        if distributed:
+            dist.destroy_process_group()
+        return
+
+    g = b200sssp.Graph.from_host(hg, "u32")
+    my_sources = sources[rank::world] if world <= NSRC else [sources[rank % NSRC]]
+    stream = torch.cuda.Stream()
+    opts = {}
+    if args.policy == "learned":
+        opts["policy"] = 1
+    # reached edges per source (TEPS numerator), measured once outside timing
+    reach = {}
+    for s in my_sources:
+        _, _, st = g.sssp(s, method=args.method, collect_reach=1, stream=stream, **opts)
+        reach[s] = (st["reached"], st["reached_edges"])
+    dist_out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    for i in range(args.warmup):
+        g.sssp(my_sources[i % len(my_sources)], method=args.method, out=dist_out, stream=stream, **opts)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    sampler.active = True
+    kernel_ms = []
+    edges = 0
+    bytes_alg = 0
+    if distributed:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    st_last = None
+    for i in range(args.steps):
+        s = my_sources[i % len(my_sources)]
+        _, _, st = g.sssp(s, method=args.method, out=dist_out, stream=stream, **opts)
+        kernel_ms.append(st["kernel_ms"])
+        nr, er = reach[s]
+        edges += er
+        bytes_alg += 8 * er + 8 * nr + 8 * g.n
+        st_last = st
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_dev = e0.elapsed_time(e1) / 1e3
+    if distributed:
+        dist.barrier()
+
+    # e2e through the public API: the graph stays resident (uploaded once, as
+    # a serving process holds it), the source id goes in by value and every
+    # step's full distance array comes back to pinned host memory.
+    h_dist = torch.empty(g.n, dtype=torch.int32, pin_memory=True)
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    e2e_edges = 0
+    for i in range(args.steps):
+        s = my_sources[i % len(my_sources)]
+        g.sssp(s, method=args.method, out=dist_out, stream=stream, **opts)
+        with torch.cuda.stream(stream):
+            h_dist.copy_(dist_out, non_blocking=True)
+        e2e_edges += reach[s][1]
+    e3.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = e2.elapsed_time(e3) / 1e3
+    sampler.active = False
+    sampler.stop()
+
+    # max over ranks
+    tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
+    tot = torch.tensor([float(edges), float(e2e_edges)], dtype=torch.float64, device="cuda")
+    if distributed:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    t_dev, t_e2e = tt.tolist()
+    edges_all, e2e_all = tot.tolist()
+
+    peak, peak_kind = load_peaks()
+    avg_kernel_s = float(np.mean(kernel_ms)) / 1e3
+    achieved = (bytes_alg / args.steps) / avg_kernel_s / 1e9
+    line = {
+        "metric": "sssp_gteps", "value": edges_all / t_dev / 1e9, "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic", "config": config,
+        "e2e": {"value": e2e_all / t_e2e / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 4 * g.n,
+                "note": "graph resident; source id passed by value; distances copied to pinned host"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": profile_traffic(), "peak_kind": peak_kind,
+                     "kernel": "k_sssp<WU32,false,kModeDelta>",
+                     "bytes_alg_per_launch": bytes_alg / args.steps,
+                     "avg_kernel_ms": avg_kernel_s * 1e3},
+        "detail": {"phases_per_solve": st_last["phases"], "buckets": st_last["iterations_used"],
+                   "delta": st_last["delta_used"], "edges_scanned_last": st_last["edges_scanned"],
+                   "reached_edges_mean": float(np.mean([v[1] for v in reach.values()])),
+                   "grid_blocks": st_last["grid_blocks"], "gen_seconds": t_gen},
+    }
+    clocks = sampler.summary()
+    line["clocks"] = clocks
+    if rank == 0 and not args.no_cpu_baseline:
+        iters, t_dij = cpu_iterations_and_dijkstra(hg, sources[0])
+        smp = cpu_reference_sample(hg, iters)
+        t_solve = smp["seconds_per_iteration"] * smp["iterations"]
+        cpu = float(np.mean([v[1] for v in reach.values()])) / t_solve / 1e9
+        line["cpu_baseline"] = {"value": cpu, "unit": "GTEPS", "cores": smp["cores"], "kind": "port",
+                                "sample": smp["sample"], "cpu_dijkstra_1core_seconds": t_dij}
+    g.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if distributed:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

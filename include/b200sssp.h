@@ -1,0 +1,237 @@
+/*
+ * b200sssp.h -- C ABI of the B200 SSSP / min-plus library (libb200sssp.so).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, never
+ * throws, and reports failure through b2_status.  Device pointers are CUDA
+ * device memory owned by the caller unless stated otherwise.  `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (charlottesylvie/rips2026-amd, paths inside
+ * that project):
+ *   b2_sssp_bf            <- bellman_ford_minplus_hip_csr
+ *                            (HIP_kernel/bellman_ford/src/bf_hip_CSR.hpp:41-66),
+ *                            _no_checks (bf_hip_no_checks_CSR.hpp:17-42),
+ *                            _var_checks (bf_var_checks.hpp:32-71),
+ *                            bellman_ford_sssp_hip
+ *                            (HIP_kernel/faster_GPU_algo/Charlotte_oneshot/sssp_hip.hpp:51-54)
+ *   b2_sssp_bf_dense      <- bellman_ford_minplus_hip
+ *                            (HIP_kernel/bellman_ford/src/bellman_ford_hip.hpp:15-60)
+ *   b2_sssp_delta         <- delta_stepping_minplus_hip_csr
+ *                            (HIP_kernel/delta_stepping/src/delta_stepping_hip_CSR.hpp:15-67)
+ *   b2_sssp_adds          <- adds_sssp_hip (Charlotte_oneshot/sssp_hip.hpp:56-59) and
+ *                            hip_adds::sssp
+ *                            (faster_GPU_algo/jasper_oneshot_untested/hip_adds_sssp.hpp:101-113)
+ *   b2_minplus_gemm_f32   <- minplus_gemm_f32 (HIP_kernel/minplus_mm/src/minplus_hip.hpp:24-33)
+ *   b2_minplus_gemm_i32   <- (int32 twin of the above; the reference is fp32 only)
+ *   b2_minplus_spgemm_f32 <- minplus_sparse::minplus_spgemm_csr_f32 / _large_rows / _tuned
+ *                            (HIP_kernel/minplus_mm/src/minplus_sparse_hip.hpp:64-150)
+ *   b2_minplus_spgemm_i32 <- (int32 twin of the above)
+ *   b2_delta_heuristic    <- choose_initial_delta (Charlotte_oneshot/sssp_hip.cpp:59-81),
+ *                            estimate_initial_delta (hip_adds_sssp.cpp:1080-1127)
+ *   b2_csrbin_read/write  <- RIPSCSR1 writer/loaders (HIP_kernel/bellman_ford/src/gr_to_csr.cpp:34-57,
+ *                            :243-278; tests/big_test.cpp:160-276)
+ */
+#ifndef B200SSSP_H_
+#define B200SSSP_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2_ABI_VERSION 1
+
+typedef enum b2_status {
+  B2_SUCCESS = 0,
+  B2_INVALID_ARGUMENT = 1, /* bad pointer, size, source, orientation, weight */
+  B2_CUDA_ERROR = 2,       /* a CUDA runtime call failed */
+  B2_OUT_OF_MEMORY = 3,
+  B2_POOL_EXHAUSTED = 4,   /* a device worklist ran out of capacity */
+  B2_BUCKET_OVERFLOW = 5,
+  B2_DEVICE_ERROR = 6,     /* a device-side consistency check failed */
+  B2_TIMEOUT = 7,          /* a bounded device wait ran out (kernel exited cleanly) */
+  B2_NOT_SUPPORTED = 8,    /* valid request outside this build's limits */
+  B2_INVALID_INDEX = 9,    /* CSR column index out of range */
+  B2_INVALID_ROWPTR = 10,  /* CSR row pointer not monotone / out of range */
+  B2_INVALID_WEIGHT = 11   /* negative / NaN weight where the method forbids it */
+} b2_status;
+
+typedef void* b2_stream; /* cudaStream_t */
+
+typedef enum b2_weight_type { B2_W_U32 = 0, B2_W_F32 = 1 } b2_weight_type;
+
+/* Incoming: row v lists edges u -> v (column u); the Bellman-Ford / delta /
+ * RIPSCSR1 convention.  Outgoing: row u lists edges u -> v; the oneshot / ADDS
+ * convention. */
+typedef enum b2_orientation { B2_INCOMING = 0, B2_OUTGOING = 1 } b2_orientation;
+
+/* Non-owning CSR view.  rowptr is int64 (rowptr_bits = 64, the
+ * minplus_sparse::Offset convention) or 32-bit (rowptr_bits = 32, the oneshot
+ * int / hip_adds uint32 convention).  colind is 32-bit.  values are uint32 or
+ * float according to weight_type. */
+typedef struct b2_csr {
+  int64_t rows;
+  int64_t cols;
+  int64_t nnz;
+  const void* rowptr;
+  const int32_t* colind;
+  const void* values;
+  int32_t rowptr_bits;
+  int32_t weight_type;
+  int32_t orientation;
+  int32_t on_device; /* 1: arrays are device pointers; 0: host pointers */
+} b2_csr;
+
+/* Resident graph: outgoing CSR packed as (dst, weight) pairs in HBM plus the
+ * solver workspace; built once, reused by every solve. */
+typedef struct b2_graph_s* b2_graph;
+
+typedef struct b2_graph_info {
+  int64_t n;
+  int64_t m;
+  int32_t weight_type;
+  int32_t max_out_degree;
+  double mean_weight;       /* over edges with weight > 0 */
+  double mean_degree;
+  size_t device_bytes;      /* graph + workspace */
+} b2_graph_info;
+
+typedef enum b2_method {
+  B2_METHOD_BF = 0,      /* frontier Bellman-Ford, Jacobi rounds (hop-exact) */
+  B2_METHOD_DELTA = 1,   /* delta-stepping, device ring buckets, one persistent launch */
+  B2_METHOD_ADDS = 2     /* asynchronous worklist (no phase barriers inside a bucket window) */
+} b2_method;
+
+typedef enum b2_bf_check {
+  B2_BF_CHECKED = 0,    /* stop at the first iteration with no change */
+  B2_BF_NO_CHECKS = 1,  /* report exactly max_iters iterations */
+  B2_BF_VAR_CHECKS = 2  /* convergence observed only every check_interval iterations */
+} b2_bf_check;
+
+typedef struct b2_sssp_opts {
+  int32_t max_iters;        /* BF: rounds (<0: n-1).  delta: buckets (<0: unbounded). */
+  int32_t bf_check;         /* b2_bf_check */
+  int32_t check_interval;   /* for B2_BF_VAR_CHECKS */
+  int32_t policy;           /* 0: fixed delta (opts.delta or the Near-Far heuristic); 1: learned */
+  double delta;             /* bucket width; <=0 selects the Near-Far heuristic */
+  double delta_scale;       /* Near-Far constant C in delta = C * mean_w / mean_deg (16) */
+  uint32_t hub_degree;      /* vertices with out-degree >= this are split into edge chunks */
+  uint32_t fusion_threshold;/* frontier size under which one block runs sub-phases alone (0 = off) */
+  float pull_fraction;      /* reserved: frontier-edge fraction for pull mode (<=0 off) */
+  uint32_t grid_blocks;     /* 0: occupancy-derived persistent grid */
+  double timeout_ms;        /* bound on every device wait (default 20000) */
+  int32_t collect_reach;    /* fill stats.reached / reached_edges (one extra O(n) pass) */
+  int32_t detect_negative_cycle; /* BF: one extra round after max_iters (python reference rule) */
+  int32_t reserved[6];
+} b2_sssp_opts;
+
+typedef struct b2_stats {
+  int32_t iterations_used;  /* BF: rounds; delta/ADDS: non-empty buckets processed */
+  int32_t converged;
+  int32_t has_negative_cycle;
+  int32_t phases;           /* barrier-separated phases executed by the persistent kernel */
+  uint64_t edges_scanned;   /* edges read during relaxation */
+  uint64_t improvements;    /* successful atomic-min updates */
+  uint64_t pushes;          /* worklist insertions */
+  uint64_t reached;         /* vertices with finite distance */
+  uint64_t reached_edges;   /* out-edges of reached vertices (TEPS numerator) */
+  double delta_used;
+  float kernel_ms;          /* device time of the persistent launch */
+  uint32_t device_error;
+  uint32_t grid_blocks;
+  uint32_t first_unchanged; /* BF: first round that changed nothing (0: none observed) */
+  uint32_t reserved[5];
+} b2_stats;
+
+/* ---- library ---------------------------------------------------------- */
+const char* b2_status_string(b2_status s);
+int b2_abi_version(void);
+void b2_sssp_opts_default(b2_sssp_opts* opts);
+/* cudaFree / cudaMemcpyAsync(D2D) for callers without their own CUDA runtime
+ * (ctypes, cgo): frees the callee-allocated SpGEMM outputs. */
+b2_status b2_device_free(void* d_ptr);
+b2_status b2_device_copy(void* d_dst, const void* d_src, size_t bytes, b2_stream stream);
+
+/* ---- resident graphs -------------------------------------------------- */
+b2_status b2_graph_create(const b2_csr* csr, b2_stream stream, b2_graph* out);
+b2_status b2_graph_destroy(b2_graph g);
+b2_status b2_graph_info_get(b2_graph g, b2_graph_info* info);
+/* Near-Far delta = scale * mean(w > 0) / mean degree (>= 1 for uint32). */
+b2_status b2_delta_heuristic(b2_graph g, double scale, double* delta_out);
+
+/* ---- SSSP -------------------------------------------------------------
+ * d_dist: n words of the graph's weight type (uint32: 0xFFFFFFFF = unreachable;
+ * float: +inf = unreachable).  d_pred: n int32 (nullable); -1 = none/source.
+ * Predecessors form a shortest-path tree when every cycle has positive weight;
+ * ties pick the smallest predecessor id. */
+b2_status b2_sssp_bf(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
+                     const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats);
+b2_status b2_sssp_delta(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
+                        const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats);
+b2_status b2_sssp_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
+                       const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats);
+/* Dense incoming adjacency (d_adj[v*n+u] = w(u->v), +inf/NaN = no edge). */
+b2_status b2_sssp_bf_dense(const float* d_adj, int32_t n, uint32_t source, float* d_dist,
+                           const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats);
+
+/* ---- min-plus products ------------------------------------------------
+ * C[i,j] = min_k A[i,k] + B[k,j], row-major with leading dimensions.
+ * f32: NaN candidates are ignored, empty min = +inf.
+ * i32: inputs must lie in [-2^30, 2^30-1]; C is clamped to <= INT32_MAX/2
+ *      (1073741823, the "missing" sentinel).  Asynchronous on `stream`. */
+b2_status b2_minplus_gemm_f32(const float* dA, const float* dB, float* dC, int32_t M,
+                              int32_t N, int32_t K, int32_t lda, int32_t ldb, int32_t ldc,
+                              b2_stream stream);
+b2_status b2_minplus_gemm_i32(const int32_t* dA, const int32_t* dB, int32_t* dC, int32_t M,
+                              int32_t N, int32_t K, int32_t lda, int32_t ldb, int32_t ldc,
+                              b2_stream stream);
+/* All-pairs shortest paths by repeated squaring of an N x N matrix in place
+ * (d_D must have a zero diagonal).  Stops early when a squaring changes
+ * nothing.  *squarings_out = products computed. */
+b2_status b2_apsp_f32(float* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
+b2_status b2_apsp_i32(int32_t* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
+
+/* CSR x CSR min-plus.  Outputs are cudaMalloc'd by the callee and owned by
+ * the caller (cudaFree).  Absent = +inf; explicit +inf / NaN entries and
+ * candidates are skipped; duplicates are min-reduced.  Output columns are
+ * sorted within each row.  A, B: on_device = 1, rowptr_bits = 64. */
+b2_status b2_minplus_spgemm_f32(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr,
+                                int32_t** dC_colind, float** dC_values, int64_t* hC_nnz,
+                                b2_stream stream);
+/* int32 values: absent = missing; entries >= INT32_MAX/2 are skipped. */
+b2_status b2_minplus_spgemm_i32(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr,
+                                int32_t** dC_colind, int32_t** dC_values, int64_t* hC_nnz,
+                                b2_stream stream);
+
+/* ---- synthetic graphs (host memory, deterministic, multi-threaded) ----- */
+typedef struct b2_host_csr {
+  int64_t n;
+  int64_t m;
+  int64_t* rowptr;   /* n+1 */
+  int32_t* colind;   /* m  */
+  uint32_t* weights; /* m  (uint32 weights) */
+  float* fweights;   /* m  (float variant, same law scaled to [0,1)) */
+} b2_host_csr;
+
+/* Outgoing CSR, columns sorted within each row, no self-loops or duplicates. */
+b2_status b2_gen_er(int64_t n, int64_t m, uint32_t wmin, uint32_t wmax, uint64_t seed,
+                    b2_host_csr* out);
+b2_status b2_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,
+                      uint32_t wmin, uint32_t wmax, uint64_t seed, b2_host_csr* out);
+b2_status b2_gen_grid(int32_t rows, int32_t cols, double shortcut_frac, double mu,
+                      double sigma, uint64_t seed, b2_host_csr* out);
+void b2_host_csr_free(b2_host_csr* g);
+/* Incoming <-> outgoing (stable: rows list columns in increasing order). */
+b2_status b2_host_csr_transpose(const b2_host_csr* in, b2_host_csr* out);
+
+/* RIPSCSR1 .csrbin (incoming CSR, float weights). */
+b2_status b2_csrbin_write(const char* path, int64_t n, int64_t nnz, const int64_t* rowptr,
+                          const int32_t* colind, const float* values);
+b2_status b2_csrbin_read(const char* path, b2_host_csr* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200SSSP_H_ */

@@ -1,0 +1,232 @@
+"""Oracle: CPU restatement of the reference algorithms -- test infrastructure.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker (or as the timed CPU baseline).  The product
+path (libb200sssp.so and the b200sssp package) never imports it.
+
+Two parts:
+  * liboracle.so (oracle.c, built by build_oracle()): Dijkstra u32/f32/f64,
+    Jacobi Bellman-Ford, dense min-plus, SpGEMM, shortest-path-tree check.
+  * numpy ports of the reference's Python path, operation for operation:
+      tropical_spmv            <- pytorch_testing/bellman_ford_attempts/Attempt1_June23/minplus_algebra.py:58-102
+      sssp_min_plus_bellman_ford <- .../Attempt1_June23/minplus_bellman_ford.py:51-102 (track_pred=False)
+      min_plus_matmul_chunked  <- pytorch_testing/matrix_mult_attempts/matrix_mult_chunked.py:1-23
+      delta_bucket_count       <- bucket_index rule, HIP_kernel/delta_stepping/src/delta_stepping_hip_CSR.cpp:233-239
+    These are what bench.py times as the reference CPU implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+SRC = os.path.join(HERE, "oracle.c")
+
+_lib = None
+
+
+def build_oracle(force: bool = False) -> str:
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        tmp = LIB + ".tmp"
+        subprocess.run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-o", tmp, SRC,
+                        "-lm"], check=True)
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build_oracle()
+        L = C.CDLL(LIB)
+        P = C.c_void_p
+        i64 = C.c_int64
+        L.orc_dijkstra_u32.argtypes = [i64, P, P, P, i64, P]
+        L.orc_dijkstra_f32.argtypes = [i64, P, P, P, i64, P]
+        L.orc_dijkstra_u32_hops.argtypes = [i64, P, P, P, i64, P, P]
+        L.orc_dijkstra_u32_hops.restype = i64
+        L.orc_dijkstra_f64.argtypes = [i64, P, P, P, i64, P]
+        L.orc_bf_jacobi_f32.argtypes = [i64, P, P, P, i64, i64, C.c_int, P, P]
+        L.orc_bf_jacobi_f64.argtypes = [i64, P, P, P, i64, i64, C.c_int, P, P]
+        L.orc_minplus_gemm_f32.argtypes = [P, P, P, i64, i64, i64, i64, i64, i64]
+        L.orc_minplus_gemm_i32.argtypes = [P, P, P, i64, i64, i64, i64, i64, i64]
+        for nm in ("orc_minplus_spgemm_f32", "orc_minplus_spgemm_i32"):
+            getattr(L, nm).argtypes = [i64, i64, i64, P, P, P, P, P, P, P, P, P, i64]
+            getattr(L, nm).restype = i64
+        L.orc_validate_spt.argtypes = [i64, P, P, P, C.c_int, i64, P, P]
+        L.orc_validate_spt.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _csr(rowptr, colind):
+    return np.ascontiguousarray(rowptr, np.int64), np.ascontiguousarray(colind, np.int32)
+
+
+def dijkstra(rowptr, colind, weights, source: int) -> np.ndarray:
+    """OUTGOING CSR.  uint32 weights -> uint32 dist (0xFFFFFFFF unreachable);
+    float32 -> float32 (+inf); float64 -> float64."""
+    rp, ci = _csr(rowptr, colind)
+    n = rp.shape[0] - 1
+    w = np.ascontiguousarray(weights)
+    if w.dtype == np.uint32:
+        d = np.empty(n, np.uint32)
+        lib().orc_dijkstra_u32(n, _p(rp), _p(ci), _p(w), source, _p(d))
+    elif w.dtype == np.float32:
+        d = np.empty(n, np.float32)
+        lib().orc_dijkstra_f32(n, _p(rp), _p(ci), _p(w), source, _p(d))
+    else:
+        w = w.astype(np.float64)
+        d = np.empty(n, np.float64)
+        lib().orc_dijkstra_f64(n, _p(rp), _p(ci), _p(w), source, _p(d))
+    return d
+
+
+def bf_iterations_u32(rowptr, colind, weights, source: int) -> tuple[int, np.ndarray]:
+    """Jacobi Bellman-Ford iteration count (max min-hop shortest path + 1) and
+    the distances, from a (dist, hops) Dijkstra on OUTGOING CSR."""
+    rp, ci = _csr(rowptr, colind)
+    n = rp.shape[0] - 1
+    w = np.ascontiguousarray(weights, np.uint32)
+    d = np.empty(n, np.uint32)
+    h = np.empty(n, np.uint32)
+    mx = lib().orc_dijkstra_u32_hops(n, _p(rp), _p(ci), _p(w), source, _p(d), _p(h))
+    return int(mx) + 1, d
+
+
+def bf_jacobi(in_rowptr, in_colind, weights, source: int, max_iters: int = -1, detect_negative: bool = False):
+    """INCOMING CSR Jacobi BF.  Returns (dist, iterations_used, converged, negative_cycle, first_unchanged)."""
+    rp, ci = _csr(in_rowptr, in_colind)
+    n = rp.shape[0] - 1
+    w = np.ascontiguousarray(weights)
+    out = np.zeros(4, np.int64)
+    if w.dtype == np.float32:
+        d = np.empty(n, np.float32)
+        lib().orc_bf_jacobi_f32(n, _p(rp), _p(ci), _p(w), source, max_iters, int(detect_negative), _p(d), _p(out))
+    else:
+        w = w.astype(np.float64)
+        d = np.empty(n, np.float64)
+        lib().orc_bf_jacobi_f64(n, _p(rp), _p(ci), _p(w), source, max_iters, int(detect_negative), _p(d), _p(out))
+    return d, int(out[0]), bool(out[1]), bool(out[2]), int(out[3])
+
+
+def minplus_gemm(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    M, K = A.shape
+    N = B.shape[1]
+    A = np.ascontiguousarray(A)
+    B = np.ascontiguousarray(B)
+    Cm = np.empty((M, N), A.dtype)
+    fn = lib().orc_minplus_gemm_f32 if A.dtype == np.float32 else lib().orc_minplus_gemm_i32
+    fn(_p(A), _p(B), _p(Cm), M, N, K, K, N, N)
+    return Cm
+
+
+def minplus_spgemm(A, B, ncols_b: int):
+    """A, B = (rowptr int64, colind int32, values f32|i32).  Returns (rowptr, colind, values), sorted rows."""
+    arp, aci = _csr(A[0], A[1])
+    brp, bci = _csr(B[0], B[1])
+    av = np.ascontiguousarray(A[2])
+    bv = np.ascontiguousarray(B[2])
+    M = arp.shape[0] - 1
+    K = brp.shape[0] - 1
+    fn = lib().orc_minplus_spgemm_f32 if av.dtype == np.float32 else lib().orc_minplus_spgemm_i32
+    nnz = fn(M, K, ncols_b, _p(arp), _p(aci), _p(av), _p(brp), _p(bci), _p(bv), None, None, None, 0)
+    crp = np.empty(M + 1, np.int64)
+    cci = np.empty(max(nnz, 1), np.int32)
+    cv = np.empty(max(nnz, 1), av.dtype)
+    fn(M, K, ncols_b, _p(arp), _p(aci), _p(av), _p(brp), _p(bci), _p(bv), _p(crp), _p(cci), _p(cv), nnz)
+    return crp, cci[:nnz], cv[:nnz]
+
+
+def validate_spt(rowptr, colind, weights, source: int, dist: np.ndarray, pred: np.ndarray) -> int:
+    rp, ci = _csr(rowptr, colind)
+    w = np.ascontiguousarray(weights)
+    kind = 0 if w.dtype == np.uint32 else 1
+    d = np.ascontiguousarray(dist, np.uint32 if kind == 0 else np.float32)
+    pr = np.ascontiguousarray(pred, np.int32)
+    return lib().orc_validate_spt(rp.shape[0] - 1, _p(rp), _p(ci), _p(w), kind, source, _p(d), _p(pr))
+
+
+# ---------------------------------------------------------------------------
+# numpy ports of the reference's Python path
+INF = np.float64(np.inf)
+
+
+def tropical_spmv(indptr: np.ndarray, indices: np.ndarray, data: np.ndarray, d: np.ndarray) -> np.ndarray:
+    """d_new[v] = min over row v of d[indices] + data (INCOMING CSR; empty rows +inf)."""
+    n = indptr.shape[0] - 1
+    if indices.shape[0] == 0:
+        return np.full(n, INF)
+    candidates = d[indices] + data
+    has = indptr[1:] > indptr[:-1]
+    out = np.full(n, INF)
+    if not np.any(has):
+        return out
+    out[has] = np.minimum.reduceat(candidates, indptr[:-1][has])
+    return out
+
+
+def sssp_min_plus_bellman_ford(indptr, indices, data, source: int, max_iters: int | None = None,
+                               iteration_hook=None):
+    """Returns (dist float64, iterations_used, converged, has_negative_cycle)."""
+    indptr = np.asarray(indptr, np.int64)
+    indices = np.asarray(indices)
+    data = np.asarray(data, np.float64)
+    n = indptr.shape[0] - 1
+    if max_iters is None:
+        max_iters = n - 1
+    d = np.full(n, INF)
+    d[source] = 0.0
+    converged = False
+    used = 0
+    for it in range(max_iters):
+        used = it + 1
+        d_new = np.minimum(d, tropical_spmv(indptr, indices, data, d))
+        if iteration_hook is not None:
+            iteration_hook(used)
+        if np.array_equal(d_new, d) or np.all(np.isclose(d_new, d) | (np.isinf(d_new) & np.isinf(d))):
+            d = d_new
+            converged = True
+            break
+        d = d_new
+    d_check = np.minimum(d, tropical_spmv(indptr, indices, data, d))
+    neg = not np.all(np.isclose(d_check, d) | (np.isinf(d_check) & np.isinf(d)))
+    return d, used, converged, neg
+
+
+def min_plus_matmul_chunked(A: np.ndarray, B: np.ndarray, block: int = 16) -> np.ndarray:
+    """C = A (min,+) B by k-blocks of broadcast add + min (the reference's chunked torch loop)."""
+    import torch
+    At = torch.from_numpy(np.ascontiguousarray(A))
+    Bt = torch.from_numpy(np.ascontiguousarray(B))
+    m, n = At.shape
+    p = Bt.shape[1]
+    Cm = torch.full((m, p), float("inf"), dtype=At.dtype)
+    for k0 in range(0, n, block):
+        k1 = min(k0 + block, n)
+        partial = At[:, k0:k1].unsqueeze(-1) + Bt[k0:k1, :].unsqueeze(0)
+        Cm = torch.minimum(Cm, partial.amin(dim=1))
+    return Cm.numpy()
+
+
+def delta_bucket_count(dist: np.ndarray, delta, weight: str) -> int:
+    """Number of distinct buckets among reached distances = the reference's
+    delta-stepping iterations_used when it converges."""
+    if weight == "u32":
+        d = np.asarray(dist, np.uint32)
+        d = d[d != 0xFFFFFFFF].astype(np.uint64)
+        return int(np.unique(d // np.uint64(int(delta))).shape[0])
+    d = np.asarray(dist, np.float32)
+    d = d[np.isfinite(d)]
+    inv = np.float32(1.0) / np.float32(delta)
+    b = np.floor(d * inv).astype(np.float64)
+    b = np.clip(b, 0, float(0x3fffffff - 1))
+    return int(np.unique(b).shape[0])

@@ -1,0 +1,249 @@
+"""b200sssp: B200-native SSSP and min-plus products (Python side).
+
+Thin host layer over the C ABI in include/b200sssp.h (libb200sssp.so built
+in-tree).  Device buffers are torch CUDA tensors; every solve runs the
+library's CUDA kernels and nothing else: there is no CPU path here.
+
+    g = b200sssp.Graph.from_host(hg)           # resident outgoing CSR
+    dist, pred, st = g.sssp(0, method="delta")  # one persistent launch
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import B2Error, LibraryMissing, check, default_opts, lib  # noqa: F401
+
+__all__ = ["HostGraph", "Graph", "gen_er", "gen_rmat", "gen_grid", "B2Error", "LibraryMissing",
+           "minplus_gemm", "apsp", "minplus_spgemm", "csrbin_read", "csrbin_write"]
+
+
+# ---------------------------------------------------------------------------
+@dataclass
+class HostGraph:
+    """CSR in host memory (numpy).  orientation: 'outgoing' or 'incoming'."""
+    n: int
+    rowptr: np.ndarray      # int64[n+1]
+    colind: np.ndarray      # int32[m]
+    weights: np.ndarray     # uint32[m]
+    fweights: np.ndarray    # float32[m]
+    orientation: str = "outgoing"
+
+    @property
+    def m(self) -> int:
+        return int(self.colind.shape[0])
+
+    def transpose(self) -> "HostGraph":
+        src = _to_hostcsr(self)
+        out = _lib.HostCSR()
+        check(lib().b2_host_csr_transpose(C.byref(src), C.byref(out)), "transpose")
+        hg = _from_hostcsr(out, "incoming" if self.orientation == "outgoing" else "outgoing")
+        return hg
+
+    def out_degree(self) -> np.ndarray:
+        if self.orientation != "outgoing":
+            raise ValueError("out_degree needs an outgoing CSR")
+        return np.diff(self.rowptr)
+
+
+def _from_hostcsr(h: _lib.HostCSR, orientation: str) -> HostGraph:
+    n, m = int(h.n), int(h.m)
+    try:
+        rowptr = np.ctypeslib.as_array(h.rowptr, shape=(n + 1,)).copy()
+        colind = np.ctypeslib.as_array(h.colind, shape=(max(m, 1),))[:m].copy()
+        w = np.ctypeslib.as_array(h.weights, shape=(max(m, 1),))[:m].copy()
+        fw = (np.ctypeslib.as_array(h.fweights, shape=(max(m, 1),))[:m].copy()
+              if bool(h.fweights) else w.astype(np.float32))
+    finally:
+        lib().b2_host_csr_free(C.byref(h))
+    return HostGraph(n, rowptr, colind, w, fw, orientation)
+
+
+def _to_hostcsr(g: HostGraph) -> _lib.HostCSR:
+    h = _lib.HostCSR()
+    h.n, h.m = g.n, g.m
+    g.rowptr = np.ascontiguousarray(g.rowptr, np.int64)
+    g.colind = np.ascontiguousarray(g.colind, np.int32)
+    g.weights = np.ascontiguousarray(g.weights, np.uint32)
+    g.fweights = np.ascontiguousarray(g.fweights, np.float32)
+    h.rowptr = g.rowptr.ctypes.data_as(C.POINTER(C.c_int64))
+    h.colind = g.colind.ctypes.data_as(C.POINTER(C.c_int32))
+    h.weights = g.weights.ctypes.data_as(C.POINTER(C.c_uint32))
+    h.fweights = g.fweights.ctypes.data_as(C.POINTER(C.c_float))
+    return h
+
+
+def gen_er(n: int, m: int, wmin: int = 1, wmax: int = 100, seed: int = 0) -> HostGraph:
+    """Directed Erdos-Renyi: m distinct arcs, no self-loops, U{wmin..wmax} weights."""
+    h = _lib.HostCSR()
+    check(lib().b2_gen_er(n, m, wmin, wmax, seed, C.byref(h)), "gen_er")
+    return _from_hostcsr(h, "outgoing")
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             wmin: int = 1, wmax: int = 255, seed: int = 0) -> HostGraph:
+    """Symmetrised RMAT (self-loops and duplicates removed), U{wmin..wmax} weights."""
+    h = _lib.HostCSR()
+    check(lib().b2_gen_rmat(scale, edge_factor, a, b, c, wmin, wmax, seed, C.byref(h)), "gen_rmat")
+    return _from_hostcsr(h, "outgoing")
+
+
+def gen_grid(rows: int, cols: int, shortcut_frac: float = 0.02, mu: float = 5.0, sigma: float = 1.0,
+             seed: int = 0) -> HostGraph:
+    """4-neighbour bidirectional grid + random long-range shortcut pairs, ceil(lognormal) weights."""
+    h = _lib.HostCSR()
+    check(lib().b2_gen_grid(rows, cols, shortcut_frac, mu, sigma, seed, C.byref(h)), "gen_grid")
+    return _from_hostcsr(h, "outgoing")
+
+
+def csrbin_write(path: str, g: HostGraph) -> None:
+    """Write an INCOMING float CSR as a RIPSCSR1 .csrbin file."""
+    if g.orientation != "incoming":
+        raise ValueError("RIPSCSR1 stores incoming CSR")
+    rp = np.ascontiguousarray(g.rowptr, np.int64)
+    ci = np.ascontiguousarray(g.colind, np.int32)
+    fv = np.ascontiguousarray(g.fweights, np.float32)
+    check(lib().b2_csrbin_write(path.encode(), g.n, g.m, rp.ctypes.data, ci.ctypes.data, fv.ctypes.data),
+          "csrbin_write")
+
+
+def csrbin_read(path: str) -> HostGraph:
+    h = _lib.HostCSR()
+    check(lib().b2_csrbin_read(path.encode(), C.byref(h)), "csrbin_read")
+    return _from_hostcsr(h, "incoming")
+
+
+# ---------------------------------------------------------------------------
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream) -> int:
+    torch = _torch()
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+_METHODS = {"bf": "b2_sssp_bf", "delta": "b2_sssp_delta", "adds": "b2_sssp_adds"}
+
+
+class Graph:
+    """A resident graph on the current CUDA device (outgoing packed CSR + workspace)."""
+
+    def __init__(self, handle: int, weight: str):
+        self._h = C.c_void_p(handle)
+        self.weight = weight
+        info = _lib.GraphInfo()
+        check(lib().b2_graph_info_get(self._h, C.byref(info)), "graph_info")
+        self.n, self.m = int(info.n), int(info.m)
+
+    @classmethod
+    def from_arrays(cls, rowptr, colind, values, *, orientation: str = "outgoing",
+                    weight: str | None = None, stream=None) -> "Graph":
+        """Arrays may be numpy (host) or torch CUDA tensors (device)."""
+        torch = _torch()
+        on_dev = isinstance(rowptr, torch.Tensor) and rowptr.is_cuda
+        keep = []
+        if on_dev:
+            rp = rowptr.contiguous(); ci = colind.contiguous().to(torch.int32); vv = values.contiguous()
+            if weight is None:
+                weight = "f32" if vv.dtype == torch.float32 else "u32"
+            if weight == "u32" and vv.dtype != torch.int32:
+                vv = vv.to(torch.int64).to(torch.int32)  # same bits for values < 2^31
+            bits = 64 if rp.dtype == torch.int64 else 32
+            keep = [rp, ci, vv]
+            ptrs = (rp.data_ptr(), ci.data_ptr(), vv.data_ptr())
+            n = rp.numel() - 1
+            nnz = ci.numel()
+        else:
+            rp = np.ascontiguousarray(rowptr)
+            bits = 64 if rp.dtype.itemsize == 8 else 32
+            rp = rp.astype(np.int64 if bits == 64 else np.uint32, copy=False)
+            ci = np.ascontiguousarray(colind, np.int32)
+            vv = np.ascontiguousarray(values)
+            if weight is None:
+                weight = "f32" if vv.dtype.kind == "f" else "u32"
+            vv = vv.astype(np.float32 if weight == "f32" else np.uint32, copy=False)
+            keep = [rp, ci, vv]
+            ptrs = (rp.ctypes.data, ci.ctypes.data, vv.ctypes.data)
+            n = rp.shape[0] - 1
+            nnz = ci.shape[0]
+        csr = _lib.CSR()
+        csr.rows = csr.cols = n
+        csr.nnz = nnz
+        csr.rowptr, csr.colind, csr.values = ptrs
+        csr.rowptr_bits = bits
+        csr.weight_type = _lib.W_F32 if weight == "f32" else _lib.W_U32
+        csr.orientation = _lib.OUTGOING if orientation == "outgoing" else _lib.INCOMING
+        csr.on_device = 1 if on_dev else 0
+        h = C.c_void_p()
+        st = _stream_ptr(stream)
+        check(lib().b2_graph_create(C.byref(csr), C.c_void_p(st), C.byref(h)), "graph_create")
+        del keep
+        return cls(h.value, weight)
+
+    @classmethod
+    def from_host(cls, g: HostGraph, weight: str = "u32", stream=None) -> "Graph":
+        vals = g.weights if weight == "u32" else g.fweights
+        return cls.from_arrays(g.rowptr, g.colind, vals, orientation=g.orientation, weight=weight,
+                               stream=stream)
+
+    def info(self) -> dict:
+        info = _lib.GraphInfo()
+        check(lib().b2_graph_info_get(self._h, C.byref(info)), "graph_info")
+        return {k: getattr(info, k) for k, _ in info._fields_}
+
+    def delta_heuristic(self, scale: float = 16.0) -> float:
+        d = C.c_double()
+        check(lib().b2_delta_heuristic(self._h, scale, C.byref(d)), "delta_heuristic")
+        return d.value
+
+    def sssp(self, source: int, method: str = "delta", pred: bool = False, out=None, out_pred=None,
+             stream=None, **opts):
+        """Run one solve; returns (dist tensor, pred tensor | None, stats dict)."""
+        torch = _torch()
+        dt = torch.float32 if self.weight == "f32" else torch.int32
+        dist = out if out is not None else torch.empty(self.n, dtype=dt, device="cuda")
+        pr = None
+        if pred:
+            pr = out_pred if out_pred is not None else torch.empty(self.n, dtype=torch.int32, device="cuda")
+        o = default_opts(**opts)
+        st = _lib.Stats()
+        fn = getattr(lib(), _METHODS[method])
+        check(fn(self._h, source, C.c_void_p(dist.data_ptr()),
+                 C.c_void_p(pr.data_ptr() if pr is not None else 0), C.byref(o),
+                 C.c_void_p(_stream_ptr(stream)), C.byref(st)), f"sssp[{method}]")
+        return dist, pr, st.as_dict()
+
+    def close(self) -> None:
+        if self._h:
+            lib().b2_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dist_to_numpy(dist, weight: str) -> np.ndarray:
+    """Device distances -> float64 numpy with +inf for unreachable."""
+    a = dist.cpu().numpy()
+    if weight == "u32":
+        u = a.view(np.uint32)
+        out = u.astype(np.float64)
+        out[u == 0xFFFFFFFF] = np.inf
+        return out
+    return a.astype(np.float64)
+
+
+# min-plus entry points are defined in .minplus (imported lazily by users)
+from .minplus import minplus_gemm, apsp, minplus_spgemm  # noqa: E402

@@ -1,0 +1,149 @@
+// Host-side internals of libb200sssp: resident graph handle, solver
+// workspace, error helpers.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/b200sssp.h"
+
+namespace b2 {
+
+#define B2_CUDA_TRY(expr)                                   \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) return ::b2::from_cuda(_e);      \
+  } while (0)
+
+inline b2_status from_cuda(cudaError_t e) {
+  if (e == cudaSuccess) return B2_SUCCESS;
+  if (e == cudaErrorMemoryAllocation) return B2_OUT_OF_MEMORY;
+  if (e == cudaErrorInvalidValue) return B2_INVALID_ARGUMENT;
+  return B2_CUDA_ERROR;
+}
+
+// Number of ring buckets in the delta-stepping window (aligned windows of
+// kRing consecutive buckets; buckets past the window go to the far pile).
+constexpr int kRing = 16;
+// Edges per hub chunk (vertices with out-degree >= hub_degree are split into
+// chunks of this many edges that any warp of the grid may take).
+constexpr uint32_t kHubChunk = 256;
+
+struct HubEntry {
+  uint32_t v;
+  uint32_t base;   // first global chunk index owned by v in this list
+};
+
+// Control block of one persistent solve (device memory).  The manager step
+// (last block to arrive at a grid barrier) is the only writer of the phase
+// record; counters are written by all blocks during a phase.
+struct PhaseRec {
+  uint32_t kind;        // PhaseKind
+  uint32_t phase;       // monotone phase id (also the near-queue dedup stamp base)
+  uint32_t fq;          // frontier queue id (QueueId)
+  uint32_t fcount;      // entries in the frontier queue
+  uint32_t push_q;      // near queue receiving same-bucket pushes
+  uint32_t stamp;       // dedup stamp for those pushes
+  uint32_t hub_in;      // hub list consumed this phase
+  uint32_t hub_in_count;
+  uint32_t hub_in_chunks;
+  uint32_t hub_out;     // hub list produced this phase
+  uint32_t cur;         // current bucket (delta)
+  uint32_t win;         // window base bucket (delta)
+  uint32_t far_sel;     // far pile being appended to (delta)
+  uint32_t iter;        // BF iteration being executed
+};
+
+enum PhaseKind : uint32_t {
+  kPhaseInit = 0,
+  kPhaseProcess = 1,   // relax a frontier (+ hub chunks of the previous phase)
+  kPhaseCommit = 2,    // BF: dist_cur[v] = dist_next[v] for v in frontier
+  kPhaseSplit = 3,     // delta: move far-pile entries into the new window
+  kPhaseProbe = 4,     // delta: count valid pending entries (max_iters cut)
+  kPhaseFinal = 5,     // write outputs
+  kPhaseDone = 6,
+};
+
+enum QueueId : uint32_t {
+  kQNear0 = 0,
+  kQNear1 = 1,
+  kQFar0 = 2,
+  kQFar1 = 3,
+  kQSlot0 = 4,   // kQSlot0 + s, s < kRing
+  kQNone = 0xFFFFFFFFu,
+};
+
+struct Control {
+  // grid barrier (must stay first; see b2_common.cuh GridBarrier)
+  uint32_t bar_arrive;
+  uint32_t bar_gen;
+  uint32_t error;
+  uint32_t error_site;
+  PhaseRec rec;
+  // counters produced during phases
+  uint32_t near_count[2];
+  uint32_t far_count[2];
+  uint32_t slot_count[kRing];
+  uint32_t far_min;        // lower bound of buckets in the active far pile
+  uint32_t far_min_next;   // exact min of the kept entries during a split
+  unsigned long long hub_packed[2];  // (entries << 36) | chunks
+  uint32_t bucket_valid;   // a valid vertex was processed in the current bucket
+  uint32_t probe_valid;    // PROBE phase result
+  // results
+  uint32_t iterations;
+  uint32_t converged;
+  uint32_t negative_cycle;
+  uint32_t phases;
+  uint32_t first_unchanged;
+  uint32_t done;
+  unsigned long long t_start;   // globaltimer at the first barrier (solve budget)
+  unsigned long long edges;
+  unsigned long long improvements;
+  unsigned long long pushes;
+};
+
+// Per-graph solver workspace, sized for n vertices (allocated on first use).
+struct Workspace {
+  size_t n = 0;
+  bool pred = false;
+  void* dist_a = nullptr;     // 4n or 8n bytes
+  void* dist_b = nullptr;     // BF second buffer
+  uint32_t* pstamp = nullptr; // near-queue dedup stamps
+  uint32_t* bstamp = nullptr; // min bucket pushed (delta)
+  uint32_t* farflag = nullptr;
+  uint32_t* queues = nullptr; // (4 + kRing) * n ids
+  HubEntry* hubs = nullptr;   // 2 * hub_cap
+  size_t hub_cap = 0;
+  Control* ctl = nullptr;
+  Control* h_ctl = nullptr;   // pinned mirror for the result read-back
+  uint32_t phase_epoch = 0;
+  size_t bytes = 0;
+};
+
+}  // namespace b2
+
+struct b2_graph_s {
+  int64_t n = 0;
+  int64_t m = 0;
+  int32_t weight_type = B2_W_U32;
+  int device = 0;
+  uint64_t* rowptr = nullptr;   // outgoing, n + 1
+  uint2* edges = nullptr;       // (dst, weight bits), m
+  uint32_t* in_rowptr32 = nullptr;  // reserved (pull mode)
+  double mean_weight = 1.0;     // over weights > 0
+  double mean_degree = 0.0;
+  int32_t max_degree = 0;
+  bool has_negative = false;
+  size_t graph_bytes = 0;
+  b2::Workspace ws;
+  std::mutex mu;   // one solve at a time per handle
+};
+
+namespace b2 {
+b2_status ensure_workspace(b2_graph g, bool pred);
+b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowptr, const uint2* edges,
+                                     int weight_type, b2_graph* out);
+}  // namespace b2

@@ -1,0 +1,936 @@
+// Persistent single-launch SSSP: frontier Bellman-Ford (Jacobi rounds) and
+// delta-stepping with device-resident ring buckets.
+//
+// One cooperative launch runs the whole solve.  Phases are separated by a
+// grid barrier whose last arriver runs a one-thread manager step (see
+// b2_common.cuh): it reads the phase's counters, picks the next phase and
+// resets consumed counters while every other block is parked.  There is no
+// host round-trip per bucket or iteration, unlike the reference
+// (delta_stepping_hip_CSR.cpp:701-780: several D2H syncs per bucket;
+// bf_hip_CSR.cpp:58-95: one sync per iteration).
+//
+// Relaxation (per phase): each warp takes 32 frontier vertices, scans their
+// out-degrees and walks the concatenated edge lists 32 edges at a time, so
+// lanes read consecutive (dst, w) pairs; the owner of an edge slot is found by
+// a 5-step shuffle binary search over the warp's inclusive degree scan.
+// Vertices with out-degree >= hub_degree are split into 256-edge chunks that
+// any warp of the grid processes in the next phase.  A relaxation is a
+// load (filter) plus one hardware atomicMin on the 32-bit key or the packed
+// 64-bit key|pred word; pushes are warp-aggregated.
+//
+// Delta-stepping bucket structure (replaces the reference's host-driven
+// current/pending/heavy queues, delta_stepping_hip_CSR.cpp:367-529):
+//   * near queues (2, ping-pong): vertices whose new distance falls in the
+//     current bucket; deduplicated per phase with a stamp word;
+//   * a window of kRing buckets [win, win + kRing), one queue each,
+//     deduplicated by a per-vertex "smallest bucket pushed" word;
+//   * a far pile for buckets past the window, one entry per vertex (flag),
+//     split into the next aligned window when the window is exhausted.
+// The bucket rule is the reference's: uint32 weights use bucket = d / delta;
+// float weights use floorf(d * (1.0f / delta)) clamped like bucket_index
+// (delta_stepping_hip_CSR.cpp:233-239).  iterations_used counts buckets in
+// which at least one vertex was settled, exactly the reference's count of
+// outer iterations.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "b2_common.cuh"
+#include "b2_internal.hpp"
+
+namespace b2 {
+
+enum Mode : int { kModeBF = 0, kModeDelta = 1 };
+constexpr int kThreads = 512;
+
+struct Params {
+  uint32_t n;
+  uint32_t source;
+  const uint64_t* __restrict__ rowptr;
+  const uint2* __restrict__ edges;
+  void* dist;        // labels receiving atomicMin (BF: round k+1 values)
+  void* dist_cur;    // BF: labels of round k (read side)
+  uint32_t* pstamp;
+  uint32_t* bstamp;
+  uint32_t* farflag;
+  uint32_t* queues;
+  HubEntry* hubs;
+  uint32_t hub_cap;
+  Control* ctl;
+  uint32_t delta_u;
+  float inv_delta;
+  uint32_t hub_degree;
+  uint32_t max_iters;
+  uint32_t phase_base;
+  uint32_t detect_negcycle;
+  unsigned long long budget_ns;
+  void* out_dist;
+  int32_t* out_pred;
+  uint32_t dist_is_out;   // `dist` aliases out_dist (no separate label buffer)
+  uint32_t is_float;
+};
+
+// ---------------------------------------------------------------------------
+// label access
+template <bool PRED>
+struct Label;
+template <>
+struct Label<false> {
+  using T = uint32_t;
+  __device__ __forceinline__ static uint32_t key(T w) { return w; }
+  __device__ __forceinline__ static T make(uint32_t key, uint32_t) { return key; }
+  static constexpr T kInf = 0xFFFFFFFFu;
+};
+template <>
+struct Label<true> {
+  using T = unsigned long long;
+  __device__ __forceinline__ static uint32_t key(T w) { return (uint32_t)(w >> 32); }
+  __device__ __forceinline__ static T make(uint32_t key, uint32_t pred) {
+    return ((unsigned long long)key << 32) | pred;
+  }
+  static constexpr T kInf = 0xFFFFFFFFFFFFFFFFull;
+};
+
+template <class W>
+__device__ __forceinline__ uint32_t bucket_of(const Params& P, uint32_t key) {
+  if (!W::kFloat) return key / P.delta_u;
+  const float d = key_to_f32(key);
+  if (!isfinite(d)) return kNoBucket;
+  const float bf = floorf(d * P.inv_delta);
+  if (bf < 0.0f) return 0;
+  if (bf >= (float)kNoBucket) return kNoBucket - 1;
+  return (uint32_t)bf;
+}
+
+__device__ __forceinline__ uint32_t* queue_ptr(const Params& P, uint32_t id) {
+  return P.queues + (size_t)id * P.n;
+}
+
+__device__ __forceinline__ void set_error(const Params& P, uint32_t code, uint32_t site) {
+  atomicCAS(&P.ctl->error, kErrNone, code);
+  atomicExch(&P.ctl->error_site, site);
+}
+
+__device__ __forceinline__ PhaseRec load_rec(const Control* c) {
+  PhaseRec r;
+  const volatile uint32_t* src = (const volatile uint32_t*)&c->rec;
+  uint32_t* dst = (uint32_t*)&r;
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(PhaseRec) / 4); ++i) dst[i] = src[i];
+  return r;
+}
+__device__ __forceinline__ void store_rec(Control* c, const PhaseRec& r) {
+  volatile uint32_t* dst = (volatile uint32_t*)&c->rec;
+  const uint32_t* src = (const uint32_t*)&r;
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(PhaseRec) / 4); ++i) dst[i] = src[i];
+}
+
+struct Tally {
+  unsigned long long edges = 0, impr = 0, pushes = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Relax one edge slot per lane and route improvements.  Must be called by all
+// 32 lanes of the warp (act = false lanes only take part in the aggregation).
+template <class W, bool PRED, int MODE>
+__device__ __forceinline__ void relax_route(const Params& P, const PhaseRec& R, bool act, uint32_t u,
+                                            uint32_t du, uint2 ed, Tally& t) {
+  using L = Label<PRED>;
+  typename L::T* lab = (typename L::T*)P.dist;
+  bool improved = false;
+  uint32_t v = 0, cand = kInfKey;
+  if (act) {
+    ++t.edges;
+    v = ed.x;
+    cand = W::extend(du, ed.y);
+    if (cand != kInfKey) {
+      const typename L::T cw = L::make(cand, u);
+      const typename L::T cur = ldcg(lab + v);
+      if (cw < cur) {
+        const typename L::T old = atomicMin(lab + v, cw);
+        improved = cand < L::key(old);
+        // (PRED: a smaller predecessor at an equal distance updates the word
+        //  but does not re-expand the vertex.)
+      }
+    }
+  }
+  if (improved) ++t.impr;
+  Control* c = P.ctl;
+  if (MODE == kModeBF) {
+    const bool want = improved && atomicExch(&P.pstamp[v], R.stamp) != R.stamp;
+    const uint32_t pos = warp_append(&c->near_count[R.push_q & 1], want);
+    if (want) {
+      if (pos < P.n) queue_ptr(P, R.push_q)[pos] = v;
+      else set_error(P, kErrQueueOverflow, 10);
+      ++t.pushes;
+    }
+    return;
+  }
+  // delta: route by bucket
+  uint32_t b = 0;
+  int cls = 0;  // 1 near, 2 window slot, 3 far
+  if (improved) {
+    b = bucket_of<W>(P, cand);
+    if (b <= R.cur) cls = 1;
+    else if (b < R.win + (uint32_t)kRing) cls = 2;
+    else cls = 3;
+  }
+  // near
+  {
+    const bool want = (cls == 1) && atomicExch(&P.pstamp[v], R.stamp) != R.stamp;
+    const uint32_t pos = warp_append(&c->near_count[R.push_q & 1], want);
+    if (want) {
+      if (pos < P.n) queue_ptr(P, R.push_q)[pos] = v;
+      else set_error(P, kErrQueueOverflow, 11);
+      ++t.pushes;
+    }
+  }
+  // window slot
+  if (__any_sync(0xffffffffu, cls == 2)) {
+    const bool want = (cls == 2) && atomicMin(&P.bstamp[v], b) > b;
+    if (want) {
+      const uint32_t s = b - R.win;
+      const uint32_t grp = __match_any_sync(__activemask(), s);
+      const uint32_t leader = __ffs(grp) - 1;
+      uint32_t base = 0;
+      if (lane_id() == leader) base = atomicAdd(&c->slot_count[s], (uint32_t)__popc(grp));
+      base = __shfl_sync(grp, base, leader);
+      const uint32_t pos = base + __popc(grp & ((1u << lane_id()) - 1u));
+      if (pos < P.n) queue_ptr(P, kQSlot0 + s)[pos] = v;
+      else set_error(P, kErrQueueOverflow, 12);
+      ++t.pushes;
+    }
+  }
+  // far pile
+  if (__any_sync(0xffffffffu, cls == 3)) {
+    bool want = false;
+    uint32_t bmin = 0xFFFFFFFFu;
+    if (cls == 3 && atomicMin(&P.bstamp[v], b) > b) {
+      bmin = b;
+      want = atomicExch(&P.farflag[v], 1u) == 0u;
+    }
+    bmin = __reduce_min_sync(0xffffffffu, bmin);
+    if (lane_id() == 0 && bmin != 0xFFFFFFFFu) atomicMin(&c->far_min, bmin);
+    const uint32_t pos = warp_append(&c->far_count[R.far_sel], want);
+    if (want) {
+      if (pos < P.n) queue_ptr(P, kQFar0 + R.far_sel)[pos] = v;
+      else set_error(P, kErrQueueOverflow, 13);
+      ++t.pushes;
+    }
+  }
+}
+
+template <class W, bool PRED, int MODE>
+__device__ __forceinline__ uint32_t src_key(const Params& P, uint32_t v) {
+  using L = Label<PRED>;
+  const typename L::T* lab = (const typename L::T*)(MODE == kModeBF ? P.dist_cur : P.dist);
+  return L::key(ldcg(lab + v));
+}
+
+// ---------------------------------------------------------------------------
+template <class W, bool PRED, int MODE>
+__device__ void process_hubs(const Params& P, const PhaseRec& R, Tally& t) {
+  const uint32_t total = R.hub_in_chunks;
+  const uint32_t cnt = min(R.hub_in_count, P.hub_cap);
+  if (cnt == 0) return;
+  const uint32_t lane = lane_id();
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t per = (total + nwarps - 1) / nwarps;
+  uint32_t c0 = gwarp * per;
+  const uint32_t c1 = min(total, c0 + per);
+  if (c0 >= c1) return;
+  const HubEntry* H = P.hubs + (size_t)(R.hub_in & 1) * P.hub_cap;
+  // last entry with base <= c0
+  uint32_t lo = 0, hi = cnt - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (ldcg(&H[mid].base) <= c0) lo = mid; else hi = mid - 1;
+  }
+  for (uint32_t j = lo; j < cnt && c0 < c1; ++j) {
+    const uint32_t v = ldcg(&H[j].v);
+    const uint32_t hb = ldcg(&H[j].base);
+    const uint32_t next = (j + 1 < cnt) ? ldcg(&H[j + 1].base) : total;
+    const uint32_t du = src_key<W, PRED, MODE>(P, v);
+    bool valid = du != kInfKey;
+    if (MODE == kModeDelta) valid = valid && bucket_of<W>(P, du) == R.cur;
+    const uint64_t beg = __ldg(&P.rowptr[v]);
+    const uint64_t end = __ldg(&P.rowptr[v + 1]);
+    for (; c0 < c1 && c0 < next; ++c0) {
+      if (!valid) continue;
+      const uint64_t e0 = beg + (uint64_t)(c0 - hb) * kHubChunk;
+      const uint64_t e1 = min(end, e0 + kHubChunk);
+      for (uint64_t eb = e0; eb < e1; eb += 32) {
+        const uint64_t e = eb + lane;
+        const bool act = e < e1;
+        uint2 ed = make_uint2(0, 0);
+        if (act) ed = __ldg(&P.edges[e]);
+        relax_route<W, PRED, MODE>(P, R, act, v, du, ed, t);
+      }
+    }
+  }
+}
+
+template <class W, bool PRED, int MODE>
+__device__ void process_frontier(const Params& P, const PhaseRec& R, Tally& t) {
+  const uint32_t* F = queue_ptr(P, R.fq);
+  const uint32_t cnt = min(R.fcount, P.n);
+  const uint32_t lane = lane_id();
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  Control* c = P.ctl;
+  for (uint32_t base = gwarp * 32; base < cnt; base += nwarps * 32) {
+    const uint32_t i = base + lane;
+    uint32_t v = 0, du = kInfKey, deg = 0;
+    uint64_t beg = 0;
+    bool valid = false;
+    if (i < cnt) {
+      v = ldcg(F + i);
+      du = src_key<W, PRED, MODE>(P, v);
+      valid = du != kInfKey;
+      if (MODE == kModeDelta) valid = valid && bucket_of<W>(P, du) == R.cur;
+      if (valid) {
+        beg = __ldg(&P.rowptr[v]);
+        const uint64_t d = __ldg(&P.rowptr[v + 1]) - beg;
+        deg = (uint32_t)min(d, (uint64_t)0xFFFFFFFFull);
+      }
+    }
+    if (MODE == kModeDelta) {
+      if (__any_sync(0xffffffffu, valid) && lane == 0 && ldcg(&c->bucket_valid) == 0)
+        c->bucket_valid = 1;
+    }
+    // hubs -> chunk list for the next phase
+    const bool hub = valid && deg >= P.hub_degree;
+    if (__any_sync(0xffffffffu, hub)) {
+      if (hub) {
+        const unsigned long long nch = (deg + kHubChunk - 1) / kHubChunk;
+        const unsigned long long old =
+            atomicAdd(&c->hub_packed[R.hub_out & 1], (1ull << 36) | nch);
+        const uint32_t pos = (uint32_t)(old >> 36);
+        const uint32_t cb = (uint32_t)(old & ((1ull << 36) - 1));
+        if (pos < P.hub_cap) {
+          HubEntry* H = P.hubs + (size_t)(R.hub_out & 1) * P.hub_cap;
+          H[pos].v = v;
+          H[pos].base = cb;
+        } else {
+          set_error(P, kErrQueueOverflow, 20);
+        }
+        deg = 0;
+      }
+    }
+    const uint32_t incl = warp_incl_scan(deg);
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t excl = incl - deg;
+    for (uint32_t eb = 0; eb < total; eb += 32) {
+      const uint32_t e = eb + lane;
+      const bool act = e < total;
+      // owner = number of lanes whose inclusive scan is <= e
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t step = 16; step >= 1; step >>= 1) {
+        const uint32_t probe = __shfl_sync(0xffffffffu, incl, j + step - 1);
+        if (probe <= e) j += step;
+      }
+      j = min(j, 31u);
+      const uint32_t o_excl = __shfl_sync(0xffffffffu, excl, j);
+      const uint32_t o_lo = __shfl_sync(0xffffffffu, (uint32_t)beg, j);
+      const uint32_t o_hi = __shfl_sync(0xffffffffu, (uint32_t)(beg >> 32), j);
+      const uint32_t o_v = __shfl_sync(0xffffffffu, v, j);
+      const uint32_t o_du = __shfl_sync(0xffffffffu, du, j);
+      uint2 ed = make_uint2(0, 0);
+      if (act) {
+        const uint64_t ebeg = ((uint64_t)o_hi << 32) | o_lo;
+        ed = __ldg(&P.edges[ebeg + (e - o_excl)]);
+      }
+      relax_route<W, PRED, MODE>(P, R, act, o_v, o_du, ed, t);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Manager steps (one thread, every other block parked at the barrier).
+__device__ __forceinline__ uint32_t vld(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+__device__ __forceinline__ unsigned long long vld64(const unsigned long long* p) {
+  return *(const volatile unsigned long long*)p;
+}
+
+template <bool PRED, int MODE>
+__device__ void manager_init(const Params& P) {
+  using L = Label<PRED>;
+  Control* c = P.ctl;
+  typename L::T* lab = (typename L::T*)P.dist;
+  // Source label: key 0 with predecessor field 0, so no equal-distance
+  // candidate can ever replace it; the output maps pred[source] to -1.
+  const uint32_t zk = P.is_float ? f32_to_key(0.0f) : 0u;
+  lab[P.source] = L::make(zk, 0u);
+  if (MODE == kModeBF) ((typename L::T*)P.dist_cur)[P.source] = L::make(zk, 0u);
+  queue_ptr(P, kQNear0)[0] = P.source;
+  c->near_count[0] = 1;
+  c->near_count[1] = 0;
+  c->far_min = 0xFFFFFFFFu;
+  c->far_min_next = 0xFFFFFFFFu;
+  c->t_start = globaltimer_ns();
+  PhaseRec r;
+  memset(&r, 0, sizeof(r));
+  r.kind = kPhaseProcess;
+  r.phase = 1;
+  r.fq = kQNear0;
+  r.fcount = 1;
+  r.push_q = kQNear1;
+  r.stamp = P.phase_base + 1;
+  r.hub_in = 1;
+  r.hub_out = 0;
+  r.cur = 0;
+  r.win = 0;
+  r.far_sel = 0;
+  r.iter = 1;
+  store_rec(c, r);
+}
+
+// Whole-solve budget: a phase sequence that outlives it ends the kernel with
+// kErrTimeout instead of looping.
+__device__ __forceinline__ bool over_budget(const Params& P, PhaseRec& nx) {
+  Control* c = P.ctl;
+  if (globaltimer_ns() - c->t_start > P.budget_ns || nx.phase > 0x7fffffffu) {
+    atomicCAS(&c->error, kErrNone, (uint32_t)kErrTimeout);
+    c->error_site = 2;
+    nx.kind = kPhaseDone;
+    store_rec(c, nx);
+    return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void consume_process_counters(Control* c, const PhaseRec& r) {
+  if (r.fq == kQNear0 || r.fq == kQNear1) c->near_count[r.fq] = 0;
+  else if (r.fq >= kQSlot0 && r.fq < kQSlot0 + kRing) c->slot_count[r.fq - kQSlot0] = 0;
+  if (r.hub_in_chunks) c->hub_packed[r.hub_in & 1] = 0ull;
+}
+
+// BF round bookkeeping.  PhaseRec.far_sel is reused as the round's role:
+// 0 = ordinary round, 2 = ordinary round whose commit precedes the
+// negative-cycle probe, 1 = the probe round (python reference: one extra
+// relaxation after max_iters, minplus_bellman_ford.py:92-99).
+__device__ void manager_bf(const Params& P) {
+  Control* c = P.ctl;
+  const PhaseRec r = load_rec(c);
+  PhaseRec nx = r;
+  nx.phase = r.phase + 1;
+  c->phases = vld(&c->phases) + 1;
+  if (r.kind == kPhaseFinal) { nx.kind = kPhaseDone; store_rec(c, nx); return; }
+  if (over_budget(P, nx)) return;
+  if (r.kind == kPhaseCommit) {
+    // frontier F_k is committed; relax it next.
+    nx.kind = kPhaseProcess;
+    nx.fq = r.fq;
+    nx.fcount = r.fcount;
+    nx.push_q = r.fq ^ 1u;
+    nx.stamp = P.phase_base + nx.phase;
+    nx.hub_in = r.hub_out ^ 1u;
+    nx.hub_in_count = 0;
+    nx.hub_in_chunks = 0;
+    nx.iter = r.iter + 1;
+    nx.far_sel = (r.far_sel == 2u) ? 1u : 0u;
+    store_rec(c, nx);
+    return;
+  }
+  // PROCESS (a relaxation round, possibly continued by a hub-only phase)
+  consume_process_counters(c, r);
+  const unsigned long long hp = vld64(&c->hub_packed[r.hub_out & 1]);
+  const uint32_t hcnt = (uint32_t)(hp >> 36);
+  const uint32_t hch = (uint32_t)(hp & ((1ull << 36) - 1));
+  if (hch > 0) {
+    nx.kind = kPhaseProcess;
+    nx.fq = kQNone;
+    nx.fcount = 0;
+    nx.hub_in = r.hub_out;
+    nx.hub_in_count = hcnt;
+    nx.hub_in_chunks = hch;
+    nx.hub_out = r.hub_out ^ 1u;
+    store_rec(c, nx);   // same round, same push queue and stamp
+    return;
+  }
+  const uint32_t nn = vld(&c->near_count[r.push_q & 1]);
+  const bool changed = nn > 0;
+  nx.hub_in_chunks = 0;
+  nx.hub_in_count = 0;
+  if (r.far_sel == 1u) {
+    c->negative_cycle = changed ? 1u : 0u;
+    nx.kind = kPhaseFinal;   // far_sel stays 1: output the committed round
+    store_rec(c, nx);
+    return;
+  }
+  c->iterations = r.iter;
+  if (!changed) {
+    c->converged = 1;
+    c->first_unchanged = r.iter;
+    nx.kind = kPhaseFinal;
+    nx.far_sel = 0u;
+    store_rec(c, nx);
+    return;
+  }
+  if (r.iter >= P.max_iters && !P.detect_negcycle) {
+    nx.kind = kPhaseFinal;
+    nx.far_sel = 0u;
+    store_rec(c, nx);
+    return;
+  }
+  nx.kind = kPhaseCommit;
+  nx.fq = r.push_q;
+  nx.fcount = nn;
+  nx.far_sel = (r.iter >= P.max_iters) ? 2u : 0u;
+  store_rec(c, nx);
+}
+
+__device__ void manager_delta(const Params& P) {
+  Control* c = P.ctl;
+  const PhaseRec r = load_rec(c);
+  PhaseRec nx = r;
+  nx.phase = r.phase + 1;
+  nx.stamp = P.phase_base + nx.phase;
+  c->phases = vld(&c->phases) + 1;
+  if (r.kind == kPhaseFinal) { nx.kind = kPhaseDone; store_rec(c, nx); return; }
+  if (over_budget(P, nx)) return;
+  if (r.kind == kPhaseProbe) {
+    c->converged = vld(&c->probe_valid) ? 0u : 1u;
+    nx.kind = kPhaseFinal;
+    store_rec(c, nx);
+    return;
+  }
+  uint32_t win = r.win;
+  uint32_t far_sel = r.far_sel;
+  uint32_t from_slot = 0;   // first window slot to look at
+  if (r.kind == kPhaseSplit) {
+    c->far_count[r.far_sel] = 0;
+    far_sel = r.far_sel ^ 1u;
+    c->far_min = vld(&c->far_min_next);
+    c->far_min_next = 0xFFFFFFFFu;
+    from_slot = 0;
+  } else {  // PROCESS
+    consume_process_counters(c, r);
+    const unsigned long long hp = vld64(&c->hub_packed[r.hub_out & 1]);
+    const uint32_t hcnt = (uint32_t)(hp >> 36);
+    const uint32_t hch = (uint32_t)(hp & ((1ull << 36) - 1));
+    const uint32_t nn = vld(&c->near_count[r.push_q & 1]);
+    if (nn > 0 || hch > 0) {
+      nx.kind = kPhaseProcess;
+      nx.fq = nn ? r.push_q : kQNone;
+      nx.fcount = nn;
+      nx.push_q = r.push_q ^ 1u;
+      nx.hub_in = r.hub_out;
+      nx.hub_in_count = hcnt;
+      nx.hub_in_chunks = hch;
+      nx.hub_out = r.hub_out ^ 1u;
+      store_rec(c, nx);
+      return;
+    }
+    // bucket r.cur is settled
+    if (vld(&c->bucket_valid)) {
+      c->iterations = vld(&c->iterations) + 1;
+      c->bucket_valid = 0;
+    }
+    if (vld(&c->iterations) >= P.max_iters) {
+      nx.kind = kPhaseProbe;
+      nx.hub_in_chunks = 0;
+      store_rec(c, nx);
+      return;
+    }
+    from_slot = r.cur - r.win + 1;
+  }
+  // next non-empty window slot
+  uint32_t cnts[kRing];
+#pragma unroll
+  for (int s = 0; s < kRing; ++s) cnts[s] = vld(&c->slot_count[s]);
+  int found = -1;
+  for (int s = (int)from_slot; s < kRing; ++s) {
+    if (cnts[s]) { found = s; break; }
+  }
+  nx.far_sel = far_sel;
+  nx.hub_in = r.hub_out;
+  nx.hub_in_count = 0;
+  nx.hub_in_chunks = 0;
+  nx.hub_out = r.hub_out ^ 1u;
+  if (found >= 0) {
+    nx.kind = kPhaseProcess;
+    nx.win = win;
+    nx.cur = win + (uint32_t)found;
+    nx.fq = kQSlot0 + (uint32_t)found;
+    nx.fcount = cnts[found];
+    nx.push_q = kQNear0;   // both near queues are empty at a bucket boundary
+    store_rec(c, nx);
+    return;
+  }
+  const uint32_t fc = vld(&c->far_count[far_sel]);
+  if (fc > 0) {
+    const uint32_t fmin = vld(&c->far_min);
+    uint32_t nwin = win + kRing;
+    const uint32_t aligned = (fmin / kRing) * kRing;
+    if (fmin != 0xFFFFFFFFu && aligned > nwin) nwin = aligned;
+    nx.kind = kPhaseSplit;
+    nx.fq = kQFar0 + far_sel;
+    nx.fcount = fc;
+    nx.win = nwin;
+    nx.cur = nwin;
+    c->far_min_next = 0xFFFFFFFFu;
+    store_rec(c, nx);
+    return;
+  }
+  c->converged = 1;
+  nx.kind = kPhaseFinal;
+  store_rec(c, nx);
+}
+
+// ---------------------------------------------------------------------------
+template <class W, bool PRED, int MODE>
+__global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
+  using L = Label<PRED>;
+  __shared__ PhaseRec s_rec;
+  Tally t;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  Control* c = P.ctl;
+
+  // INIT: all labels unreached; delta bucket stamps / far flags cleared.
+  for (size_t v = tid; v < P.n; v += stride) {
+    ((typename L::T*)P.dist)[v] = L::kInf;
+    if (MODE == kModeBF) ((typename L::T*)P.dist_cur)[v] = L::kInf;
+    if (MODE == kModeDelta) {
+      P.bstamp[v] = 0xFFFFFFFFu;
+      P.farflag[v] = 0u;
+    }
+  }
+  bool ok = grid_barrier((GridBarrier*)c, gridDim.x, P.budget_ns, [&] { manager_init<PRED, MODE>(P); });
+  while (ok) {
+    if (threadIdx.x == 0) s_rec = load_rec(c);
+    __syncthreads();
+    PhaseRec R = s_rec;
+    if (R.kind == kPhaseDone) break;
+    R.fcount = min(R.fcount, P.n);
+    if (R.kind == kPhaseProcess) {
+      if (R.hub_in_chunks) process_hubs<W, PRED, MODE>(P, R, t);
+      if (R.fcount) process_frontier<W, PRED, MODE>(P, R, t);
+    } else if (R.kind == kPhaseCommit) {
+      const uint32_t* F = queue_ptr(P, R.fq);
+      for (size_t i = tid; i < R.fcount; i += stride) {
+        const uint32_t v = ldcg(F + i);
+        ((typename L::T*)P.dist_cur)[v] = ldcg((const typename L::T*)P.dist + v);
+      }
+    } else if (R.kind == kPhaseSplit) {
+      const uint32_t* F = queue_ptr(P, R.fq);
+      uint32_t kmin = 0xFFFFFFFFu;
+      for (size_t base = tid - lane_id(); base < R.fcount; base += stride) {
+        const size_t i = base + lane_id();
+        int cls = 0;
+        uint32_t v = 0, b = 0;
+        if (i < R.fcount) {
+          v = ldcg(F + i);
+          const uint32_t k = L::key(ldcg((const typename L::T*)P.dist + v));
+          b = bucket_of<W>(P, k);
+          if (b < R.win) { cls = 0; P.farflag[v] = 0u; }
+          else if (b < R.win + (uint32_t)kRing) { cls = 2; P.farflag[v] = 0u; }
+          else { cls = 3; kmin = min(kmin, b); }
+        }
+        if (cls == 2) {
+          const uint32_t s = b - R.win;
+          const uint32_t grp = __match_any_sync(__activemask(), s);
+          const uint32_t leader = __ffs(grp) - 1;
+          uint32_t bs = 0;
+          if (lane_id() == leader) bs = atomicAdd(&c->slot_count[s], (uint32_t)__popc(grp));
+          bs = __shfl_sync(grp, bs, leader);
+          const uint32_t pos = bs + __popc(grp & ((1u << lane_id()) - 1u));
+          if (pos < P.n) queue_ptr(P, kQSlot0 + s)[pos] = v;
+          else set_error(P, kErrQueueOverflow, 30);
+        }
+        const uint32_t pos = warp_append(&c->far_count[R.far_sel ^ 1u], cls == 3);
+        if (cls == 3) {
+          if (pos < P.n) queue_ptr(P, kQFar0 + (R.far_sel ^ 1u))[pos] = v;
+          else set_error(P, kErrQueueOverflow, 31);
+        }
+      }
+      kmin = __reduce_min_sync(0xffffffffu, kmin);
+      if (lane_id() == 0 && kmin != 0xFFFFFFFFu) atomicMin(&c->far_min_next, kmin);
+    } else if (R.kind == kPhaseProbe) {
+      bool any = false;
+      const uint32_t first = R.cur - R.win + 1;
+      for (uint32_t s = first; s < (uint32_t)kRing && !any; ++s) {
+        const uint32_t cnt = ldcg(&c->slot_count[s]);
+        const uint32_t* F = queue_ptr(P, kQSlot0 + s);
+        for (size_t i = tid; i < cnt; i += stride) {
+          const uint32_t v = ldcg(F + i);
+          const uint32_t k = L::key(ldcg((const typename L::T*)P.dist + v));
+          if (k != kInfKey && bucket_of<W>(P, k) == R.win + s) { any = true; break; }
+        }
+      }
+      {
+        const uint32_t cnt = ldcg(&c->far_count[R.far_sel]);
+        const uint32_t* F = queue_ptr(P, kQFar0 + R.far_sel);
+        for (size_t i = tid; i < cnt && !any; i += stride) {
+          const uint32_t v = ldcg(F + i);
+          const uint32_t k = L::key(ldcg((const typename L::T*)P.dist + v));
+          if (k != kInfKey && bucket_of<W>(P, k) >= R.win + (uint32_t)kRing) any = true;
+        }
+      }
+      if (any) c->probe_valid = 1u;
+    } else if (R.kind == kPhaseFinal) {
+      // far_sel == 1 (BF probe round): the answer is the committed round.
+      const typename L::T* src =
+          (const typename L::T*)((MODE == kModeBF && R.far_sel == 1u) ? P.dist_cur : P.dist);
+      for (size_t v = tid; v < P.n; v += stride) {
+        const typename L::T wv = ldcg(src + v);
+        const uint32_t k = L::key(wv);
+        if (W::kFloat) {
+          ((float*)P.out_dist)[v] = (k == kInfKey) ? __uint_as_float(0x7f800000u) : key_to_f32(k);
+        } else if (!P.dist_is_out || (const void*)src != P.out_dist) {
+          ((uint32_t*)P.out_dist)[v] = k;
+        }
+        if (PRED && P.out_pred) {
+          int32_t pr = -1;
+          if (k != kInfKey && v != P.source) pr = (int32_t)(uint32_t)(wv & 0xFFFFFFFFull);
+          P.out_pred[v] = pr;
+        }
+      }
+    }
+    if (MODE == kModeBF) {
+      ok = grid_barrier((GridBarrier*)c, gridDim.x, P.budget_ns, [&] { manager_bf(P); });
+    } else {
+      ok = grid_barrier((GridBarrier*)c, gridDim.x, P.budget_ns, [&] { manager_delta(P); });
+    }
+  }
+  // flush tallies (one atomic per warp)
+  unsigned long long e = t.edges, im = t.impr, pu = t.pushes;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_down_sync(0xffffffffu, e, o);
+    im += __shfl_down_sync(0xffffffffu, im, o);
+    pu += __shfl_down_sync(0xffffffffu, pu, o);
+  }
+  if (lane_id() == 0) {
+    if (e) atomicAdd(&c->edges, e);
+    if (im) atomicAdd(&c->improvements, im);
+    if (pu) atomicAdd(&c->pushes, pu);
+  }
+}
+
+// Reached vertices and their out-edges (the TEPS numerator).
+template <bool PRED>
+__global__ void k_reach(uint32_t n, const uint64_t* rowptr, const void* labels, int is_float,
+                        unsigned long long* out) {
+  unsigned long long r = 0, re = 0;
+  for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x) {
+    bool reached;
+    if (PRED) reached = (((const unsigned long long*)labels)[v] >> 32) != 0xFFFFFFFFull;
+    else if (is_float) reached = isfinite(((const float*)labels)[v]);
+    else reached = ((const uint32_t*)labels)[v] != 0xFFFFFFFFu;
+    if (reached) { ++r; re += rowptr[v + 1] - rowptr[v]; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    r += __shfl_down_sync(0xffffffffu, r, o);
+    re += __shfl_down_sync(0xffffffffu, re, o);
+  }
+  if ((threadIdx.x & 31) == 0) { atomicAdd(&out[0], r); atomicAdd(&out[1], re); }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+template <class W, bool PRED, int MODE>
+int max_grid() {
+  static int cached = 0;
+  if (cached) return cached;
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sssp<W, PRED, MODE>, kThreads, 0);
+  if (per < 1) per = 1;
+  cached = per * sms;
+  return cached;
+}
+
+template <class W, bool PRED, int MODE>
+cudaError_t launch(const Params& P, int grid, cudaStream_t st) {
+  Params copy = P;
+  void* args[] = {&copy};
+  return cudaLaunchCooperativeKernel((void*)k_sssp<W, PRED, MODE>, dim3(grid), dim3(kThreads), args, 0, st);
+}
+
+b2_status map_device_error(uint32_t e) {
+  switch (e) {
+    case kErrNone: return B2_SUCCESS;
+    case kErrTimeout: return B2_TIMEOUT;
+    case kErrQueueOverflow: return B2_POOL_EXHAUSTED;
+    default: return B2_DEVICE_ERROR;
+  }
+}
+
+b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t* d_pred,
+                   const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats) {
+  if (!g || !d_dist) return B2_INVALID_ARGUMENT;
+  if ((int64_t)source >= g->n) return B2_INVALID_ARGUMENT;
+  b2_sssp_opts o;
+  if (o_in) o = *o_in; else b2_sssp_opts_default(&o);
+  if (mode == kModeDelta && g->has_negative) return B2_INVALID_WEIGHT;
+  const bool isf = g->weight_type == B2_W_F32;
+  const bool pred = d_pred != nullptr;
+  std::lock_guard<std::mutex> lock(g->mu);
+  b2_status s = ensure_workspace(g, pred);
+  if (s != B2_SUCCESS) return s;
+  Workspace& w = g->ws;
+
+  Params P;
+  memset(&P, 0, sizeof(P));
+  P.n = (uint32_t)g->n;
+  P.source = source;
+  P.rowptr = g->rowptr;
+  P.edges = g->edges;
+  P.pstamp = w.pstamp;
+  P.bstamp = w.bstamp;
+  P.farflag = w.farflag;
+  P.queues = w.queues;
+  P.hubs = w.hubs;
+  P.hub_cap = (uint32_t)w.hub_cap;
+  P.ctl = w.ctl;
+  P.hub_degree = std::max<uint32_t>(32u, o.hub_degree ? o.hub_degree : 256u);
+  P.out_dist = d_dist;
+  P.out_pred = d_pred;
+  P.is_float = isf ? 1u : 0u;
+  P.budget_ns = (unsigned long long)(std::max(1.0, o.timeout_ms > 0 ? o.timeout_ms : 20000.0) * 1.0e6);
+  // label buffers
+  if (pred) {
+    P.dist = w.dist_a;
+    P.dist_cur = w.dist_b;
+    P.dist_is_out = 0;
+  } else {
+    P.dist = d_dist;        // keys are built in the caller's buffer, converted in place
+    P.dist_cur = w.dist_b;
+    P.dist_is_out = 1;
+  }
+  double delta = 1.0;
+  if (mode == kModeBF) {
+    int64_t mi = o.max_iters < 0 ? g->n - 1 : o.max_iters;
+    if (mi > 0x7fffffff) mi = 0x7fffffff;
+    P.max_iters = (uint32_t)mi;
+    P.detect_negcycle = o.detect_negative_cycle ? 1u : 0u;
+    // the zero key of the weight type is chosen in manager_init from these:
+    P.inv_delta = 1.0f;
+    P.delta_u = 1u;
+  } else {
+    delta = o.delta;
+    if (!(delta > 0.0)) b2_delta_heuristic(g, o.delta_scale > 0 ? o.delta_scale : 16.0, &delta);
+    if (isf) {
+      const float df = (float)delta;
+      if (!(df > 0.0f) || !std::isfinite(df)) return B2_INVALID_ARGUMENT;
+      P.inv_delta = 1.0f / df;
+      P.delta_u = 1u;
+    } else {
+      const double dd = std::max(1.0, std::floor(delta));
+      P.delta_u = (uint32_t)std::min(dd, 4294967295.0);
+      P.inv_delta = 0.0f;
+      delta = (double)P.delta_u;
+    }
+    P.max_iters = o.max_iters < 0 ? 0xFFFFFFFFu : (uint32_t)o.max_iters;
+  }
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->delta_used = delta;
+  }
+  // zero iterations: only the source is reached (reference loop never runs)
+  if (P.max_iters == 0) {
+    // labels: fill via a tiny kernel-free path
+    if (isf) {
+      std::vector<float> h((size_t)g->n, INFINITY);
+      h[source] = 0.0f;
+      B2_CUDA_TRY(cudaMemcpyAsync(d_dist, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st));
+    } else {
+      std::vector<uint32_t> h((size_t)g->n, 0xFFFFFFFFu);
+      h[source] = 0u;
+      B2_CUDA_TRY(cudaMemcpyAsync(d_dist, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    if (pred) B2_CUDA_TRY(cudaMemsetAsync(d_pred, 0xFF, (size_t)g->n * 4, st));
+    B2_CUDA_TRY(cudaStreamSynchronize(st));
+    return B2_SUCCESS;
+  }
+  // phase stamps never repeat across solves on this workspace
+  if (w.phase_epoch > 0xF0000000u) {
+    B2_CUDA_TRY(cudaMemsetAsync(w.pstamp, 0, (size_t)g->n * 4, st));
+    w.phase_epoch = 1;
+  }
+  P.phase_base = w.phase_epoch;
+
+  int grid;
+  cudaError_t e;
+  B2_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(Control), st));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+#define B2_LAUNCH(WT, PR, MD)                                              \
+  do {                                                                     \
+    grid = max_grid<WT, PR, MD>();                                         \
+    if (o.grid_blocks && (int)o.grid_blocks < grid) grid = o.grid_blocks;  \
+    e = launch<WT, PR, MD>(P, grid, st);                                   \
+  } while (0)
+  if (mode == kModeBF) {
+    if (isf) { if (pred) B2_LAUNCH(WF32, true, kModeBF); else B2_LAUNCH(WF32, false, kModeBF); }
+    else { if (pred) B2_LAUNCH(WU32, true, kModeBF); else B2_LAUNCH(WU32, false, kModeBF); }
+  } else {
+    if (isf) { if (pred) B2_LAUNCH(WF32, true, kModeDelta); else B2_LAUNCH(WF32, false, kModeDelta); }
+    else { if (pred) B2_LAUNCH(WU32, true, kModeDelta); else B2_LAUNCH(WU32, false, kModeDelta); }
+  }
+#undef B2_LAUNCH
+  cudaEventRecord(e1, st);
+  if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return from_cuda(e); }
+  e = cudaMemcpyAsync(w.h_ctl, w.ctl, sizeof(Control), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return from_cuda(e);
+  const Control& hc = *w.h_ctl;
+  w.phase_epoch += hc.rec.phase + 2;
+  b2_status ds = map_device_error(hc.error);
+  if (stats) {
+    stats->iterations_used = (int32_t)hc.iterations;
+    stats->converged = (int32_t)hc.converged;
+    stats->has_negative_cycle = (int32_t)hc.negative_cycle;
+    stats->phases = (int32_t)hc.phases;
+    stats->edges_scanned = hc.edges;
+    stats->improvements = hc.improvements;
+    stats->pushes = hc.pushes;
+    stats->kernel_ms = ms;
+    stats->device_error = hc.error;
+    stats->grid_blocks = (uint32_t)grid;
+    stats->first_unchanged = hc.first_unchanged;
+  }
+  if (ds != B2_SUCCESS) return ds;
+  if (stats && o.collect_reach) {
+    unsigned long long* d_r = nullptr;
+    B2_CUDA_TRY(cudaMalloc((void**)&d_r, 16));
+    cudaMemsetAsync(d_r, 0, 16, st);
+    const void* lab = pred ? w.dist_a : d_dist;
+    if (pred) k_reach<true><<<1024, 256, 0, st>>>(P.n, g->rowptr, lab, isf, d_r);
+    else k_reach<false><<<1024, 256, 0, st>>>(P.n, g->rowptr, lab, isf, d_r);
+    unsigned long long hr[2] = {0, 0};
+    cudaMemcpyAsync(hr, d_r, 16, cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    cudaFree(d_r);
+    if (e != cudaSuccess) return from_cuda(e);
+    stats->reached = hr[0];
+    stats->reached_edges = hr[1];
+  }
+  return B2_SUCCESS;
+}
+
+}  // namespace b2
+
+using namespace b2;
+
+extern "C" b2_status b2_sssp_bf(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
+                                const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats) {
+  return run_sssp(g, kModeBF, source, d_dist, d_pred, opts, (cudaStream_t)stream, stats);
+}
+
+extern "C" b2_status b2_sssp_delta(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
+                                   const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats) {
+  return run_sssp(g, kModeDelta, source, d_dist, d_pred, opts, (cudaStream_t)stream, stats);
+}

@@ -1,0 +1,233 @@
+"""GPU parity: Bellman-Ford and delta-stepping kernels vs the oracle.
+
+Distances must be bit-exact (uint32 and float32: the float fixpoint of
+relaxation is unique, so a float32 Dijkstra reproduces it); against the
+reference's float64 python path float32 results agree within 1e-6 relative.
+Iteration counts follow the reference's rules exactly.  Predecessor arrays are
+checked as shortest-path trees.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+INF_U = 0xFFFFFFFF
+
+
+def _graph(b2, hg, weight):
+    return b2.Graph.from_host(hg, weight=weight)
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+def _dist_u32(t):
+    return _np(t).view(np.uint32)
+
+
+def _gpu_vs_dijkstra(b2, orc, hg, weight, sources, method="delta", pred=False, **opts):
+    g = _graph(b2, hg, weight)
+    w = hg.weights if weight == "u32" else hg.fweights
+    for s in sources:
+        dist, pr, st = g.sssp(int(s), method=method, pred=pred, **opts)
+        ref = orc.dijkstra(hg.rowptr, hg.colind, w, int(s))
+        got = _dist_u32(dist) if weight == "u32" else _np(dist)
+        assert np.array_equal(got, ref), (method, weight, s, int(np.sum(got != ref)))
+        if pred:
+            code = orc.validate_spt(hg.rowptr, hg.colind, w, int(s), got, _np(pr))
+            assert code == 0, (method, weight, s, code)
+        yield got, st
+    g.close()
+
+
+@pytest.mark.parametrize("weight", ["u32", "f32"])
+@pytest.mark.parametrize("method", ["bf", "delta"])
+def test_er_c1_exact(b2, orc, cuda, weight, method):
+    hg = b2.gen_er(4096, 32768, 1, 100, 0)
+    for _ in _gpu_vs_dijkstra(b2, orc, hg, weight, [0, 1, 4095], method=method):
+        pass
+
+
+def test_c1_matches_reference_python_bf(b2, golden, cuda):
+    z = golden("bf_py.npz")
+    hg = b2.gen_er(4096, 32768, 1, 100, 0)
+    g = _graph(b2, hg, "u32")
+    for method in ("bf", "delta"):
+        dist, _, st = g.sssp(0, method=method)
+        d = _dist_u32(dist).astype(np.float64)
+        d[_dist_u32(dist) == INF_U] = np.inf
+        assert np.array_equal(d, z["c1_er4096/dist"]), method
+    dist, _, st = g.sssp(0, method="bf")
+    assert st["iterations_used"] == int(z["c1_er4096/meta"][3]) and st["converged"] == 1
+
+
+@pytest.mark.parametrize("weight", ["u32", "f32"])
+@pytest.mark.parametrize("method", ["bf", "delta"])
+def test_rmat_and_grid_exact_with_pred(b2, orc, cuda, weight, method):
+    for hg in (b2.gen_rmat(13, 16, seed=2), b2.gen_grid(96, 80, 0.02, seed=3)):
+        deg = np.diff(hg.rowptr)
+        srcs = [int(np.argmax(deg)), int(np.nonzero(deg)[0][7]), 0 if deg[0] else int(np.nonzero(deg)[0][0])]
+        for _ in _gpu_vs_dijkstra(b2, orc, hg, weight, srcs, method=method, pred=True):
+            pass
+
+
+@pytest.mark.parametrize("delta", [1, 3, 40, 255, 100000])
+def test_delta_bucket_counts_and_windows(b2, orc, cuda, delta):
+    hg = b2.gen_rmat(12, 8, seed=5)
+    for got, st in _gpu_vs_dijkstra(b2, orc, hg, "u32", [int(np.argmax(np.diff(hg.rowptr)))], delta=float(delta)):
+        assert st["iterations_used"] == orc.delta_bucket_count(got, delta, "u32")
+        assert st["converged"] == 1
+
+
+@pytest.mark.parametrize("delta", [0.003, 0.05, 0.7, 9.0])
+def test_delta_float_bucket_rule(b2, orc, cuda, delta):
+    hg = b2.gen_grid(48, 40, 0.02, seed=8)
+    for got, st in _gpu_vs_dijkstra(b2, orc, hg, "f32", [5], delta=delta):
+        assert st["iterations_used"] == orc.delta_bucket_count(got, np.float32(delta), "f32")
+
+
+def test_delta_max_iters_partial_state(b2, orc, cuda):
+    """After k buckets: vertices of the first k buckets are final, every other
+    vertex holds min over settled u of d[u] + w (reference loop semantics,
+    delta_stepping_hip_CSR.cpp:701-780)."""
+    hg = b2.gen_er(2000, 12000, 1, 60, 4)
+    g = _graph(b2, hg, "u32")
+    final = orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 0)
+    delta = 16
+    fin = final[final != INF_U].astype(np.int64)
+    buckets = np.unique(fin // delta)
+    for k in (1, 2, 5, len(buckets) - 1, len(buckets), len(buckets) + 3):
+        dist, _, st = g.sssp(0, method="delta", delta=float(delta), max_iters=k)
+        got = _dist_u32(dist)
+        settled_b = set(buckets[:k].tolist())
+        settled = np.array([d != INF_U and (int(d) // delta) in settled_b for d in final])
+        exp = np.full(hg.n, INF_U, np.uint64)
+        exp[settled] = final[settled]
+        src = np.repeat(np.arange(hg.n), np.diff(hg.rowptr))
+        msk = settled[src]
+        cand = final[src[msk]].astype(np.uint64) + hg.weights[msk]
+        dst = hg.colind[msk]
+        np.minimum.at(exp, dst, np.minimum(cand, INF_U))
+        exp[settled] = final[settled]
+        assert np.array_equal(got, exp.astype(np.uint32)), k
+        assert st["iterations_used"] == min(k, len(buckets))
+        assert st["converged"] == (1 if k >= len(buckets) else 0)
+
+
+def test_bf_iterations_hop_limits_and_negative_weights(b2, orc, golden, cuda):
+    z = golden("bf_py.npz")
+    for name in [str(x) for x in z["names"]]:
+        if name == "c1_er4096":
+            continue
+        n, src, mi, iters, conv, neg = (int(x) for x in z[f"{name}/meta"])
+        rp, ci, dv = z[f"{name}/rowptr"], z[f"{name}/colind"], z[f"{name}/data"]
+        dv32 = dv.astype(np.float32)
+        g = b2.Graph.from_arrays(rp, ci, dv32, orientation="incoming", weight="f32")
+        dist, _, st = g.sssp(src, method="bf", max_iters=mi, detect_negative_cycle=1)
+        got = _np(dist)
+        od, oused, oconv, oneg, _ = orc.bf_jacobi(rp, ci, dv32, src, mi, detect_negative=True)
+        assert np.array_equal(got, od), name
+        assert st["iterations_used"] == oused == iters, name
+        assert bool(st["converged"]) == oconv == bool(conv), name
+        assert bool(st["has_negative_cycle"]) == oneg == bool(neg), name
+        ref = z[f"{name}/dist"]
+        fin = np.isfinite(ref)
+        assert np.array_equal(np.isfinite(got), fin), name
+        if not neg:
+            assert np.allclose(got[fin], ref[fin], rtol=1e-6, atol=1e-5), name
+        g.close()
+
+
+def test_dense_known_answers_on_gpu_bf(b2, golden, cuda):
+    z = golden("dense_kats.npz")
+    for name in [str(x) for x in z["names"]]:
+        n, src, py_iters = (int(x) for x in z[f"{name}/meta"])
+        e = z[f"{name}/edges"]
+        if e.shape[0]:
+            order = np.lexsort((e[:, 0], e[:, 1]))
+            e = e[order]
+        rp = np.zeros(n + 1, np.int64)
+        np.add.at(rp, e[:, 1].astype(np.int64) + 1, 1)
+        rp = np.cumsum(rp)
+        g = b2.Graph.from_arrays(rp, e[:, 0].astype(np.int32), e[:, 2].astype(np.float32),
+                                 orientation="incoming", weight="f32")
+        dist, _, st = g.sssp(src, method="bf")
+        got = _np(dist).astype(np.float64)
+        exp = z[f"{name}/expected"]
+        both = np.isinf(got) & np.isinf(exp)
+        with np.errstate(invalid="ignore"):
+            ok = both | (np.abs(got - exp) <= 1e-4 * (1 + np.abs(got) + np.abs(exp)))
+        assert ok.all(), name
+        if n > 1:
+            assert st["iterations_used"] == py_iters, name
+        g.close()
+
+
+def test_variants_no_checks_and_single_vertex(b2, cuda):
+    g = b2.Graph.from_arrays(np.array([0, 0], np.int64), np.zeros(0, np.int32), np.zeros(0, np.uint32))
+    dist, _, st = g.sssp(0, method="bf")
+    assert _dist_u32(dist).tolist() == [0] and st["iterations_used"] == 0 and st["converged"] == 0
+    dist, _, st = g.sssp(0, method="delta")
+    assert _dist_u32(dist).tolist() == [0]
+
+
+def test_unreachable_zero_weights_duplicates(b2, orc, cuda):
+    # duplicate arcs 0->1 (9, 3), zero-weight arcs 0->2 and 1->3, isolated vertex 5
+    rp = np.array([0, 3, 4, 5, 5, 5, 5], np.int64)
+    ci = np.array([1, 1, 2, 3, 4], np.int32)
+    w = np.array([9, 3, 0, 0, 7], np.uint32)
+    for method in ("bf", "delta"):
+        g = b2.Graph.from_arrays(rp, ci, w)
+        dist, pr, _ = g.sssp(0, method=method, pred=True)
+        assert _dist_u32(dist).tolist() == [0, 3, 0, 3, 7, INF_U], method
+        assert _np(pr).tolist() == [-1, 0, 0, 1, 2, -1], method
+
+
+def test_incoming_orientation_same_answer(b2, orc, cuda):
+    hg = b2.gen_rmat(11, 8, seed=9)
+    hg.weights = (hg.weights * 3 + np.arange(hg.m, dtype=np.uint32) % 7).astype(np.uint32)  # asymmetric
+    gi = hg.transpose()
+    a = b2.Graph.from_host(hg, "u32")
+    b = b2.Graph.from_arrays(gi.rowptr, gi.colind, gi.weights, orientation="incoming", weight="u32")
+    for method in ("bf", "delta"):
+        da, _, _ = a.sssp(3, method=method)
+        db, _, _ = b.sssp(3, method=method)
+        assert np.array_equal(_dist_u32(da), _dist_u32(db))
+        assert np.array_equal(_dist_u32(da), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 3))
+
+
+def test_invalid_inputs_rejected(b2, cuda):
+    with pytest.raises(b2.B2Error) as e:
+        b2.Graph.from_arrays(np.array([0, 2, 1], np.int64), np.array([1, 0], np.int32), np.array([1, 1], np.uint32))
+    assert e.value.status == 10  # INVALID_ROWPTR
+    with pytest.raises(b2.B2Error) as e:
+        b2.Graph.from_arrays(np.array([0, 1, 2], np.int64), np.array([1, 5], np.int32), np.array([1, 1], np.uint32))
+    assert e.value.status == 9   # INVALID_INDEX
+    with pytest.raises(b2.B2Error) as e:
+        b2.Graph.from_arrays(np.array([0, 1, 1], np.int64), np.array([1], np.int32), np.array([np.nan], np.float32))
+    assert e.value.status == 11  # INVALID_WEIGHT
+    g = b2.Graph.from_arrays(np.array([0, 1, 1], np.int64), np.array([1], np.int32), np.array([-1.0], np.float32))
+    with pytest.raises(b2.B2Error) as e:
+        g.sssp(0, method="delta")
+    assert e.value.status == 11  # delta needs nonnegative weights
+    d, _, _ = g.sssp(0, method="bf")
+    assert _np(d).tolist() == [0.0, -1.0]
+    with pytest.raises(b2.B2Error):
+        g.sssp(7, method="bf")
+
+
+def test_repeatable_and_large_properties(b2, orc, cuda):
+    hg = b2.gen_rmat(17, 16, seed=11)
+    g = _graph(b2, hg, "u32")
+    s = int(np.argmax(np.diff(hg.rowptr)))
+    d1, p1, st1 = g.sssp(s, method="delta", pred=True, collect_reach=1)
+    d2, p2, _ = g.sssp(s, method="delta", pred=True)
+    d3, _, _ = g.sssp(s, method="bf")
+    assert np.array_equal(_np(d1), _np(d2)) and np.array_equal(_np(p1), _np(p2))
+    assert np.array_equal(_np(d1), _np(d3))
+    ref = orc.dijkstra(hg.rowptr, hg.colind, hg.weights, s)
+    assert np.array_equal(_dist_u32(d1), ref)
+    reached = ref != INF_U
+    assert st1["reached"] == int(reached.sum())
+    assert st1["reached_edges"] == int(np.diff(hg.rowptr)[reached].sum())
