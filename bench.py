@@ -199,6 +199,7 @@ def main():
     ap.add_argument("--policy", default="fixed", choices=["fixed", "learned"])
     ap.add_argument("--method", default="delta", choices=["delta", "bf", "adds"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--trace-out", default=None, help="write one traced solve's phase list (JSON)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -306,6 +307,11 @@ def main():
     t_dev, t_e2e = tt.tolist()
     edges_all, e2e_all = tot.tolist()
 
+    if args.trace_out and rank == 0:
+        _, _, stt = g.sssp(my_sources[0], method=args.method, out=dist_out, stream=stream, trace=1, **opts)
+        with open(args.trace_out, "w") as f:
+            json.dump({"stats": stt, "phases": g.trace()}, f)
+
     peak, peak_kind = load_peaks()
     avg_kernel_s = float(np.mean(kernel_ms)) / 1e3
     achieved = (bytes_alg / args.steps) / avg_kernel_s / 1e9
@@ -325,6 +331,7 @@ def main():
                      "avg_kernel_ms": avg_kernel_s * 1e3},
         "detail": {"phases_per_solve": st_last["phases"], "buckets": st_last["iterations_used"],
                    "delta": st_last["delta_used"], "edges_scanned_last": st_last["edges_scanned"],
+                   "improvements_last": st_last["improvements"], "pushes_last": st_last["pushes"],
                    "reached_edges_mean": float(np.mean([v[1] for v in reach.values()])),
                    "grid_blocks": st_last["grid_blocks"], "gen_seconds": t_gen},
     }

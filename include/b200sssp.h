@@ -124,8 +124,19 @@ typedef struct b2_sssp_opts {
   double timeout_ms;        /* bound on every device wait (default 20000) */
   int32_t collect_reach;    /* fill stats.reached / reached_edges (one extra O(n) pass) */
   int32_t detect_negative_cycle; /* BF: one extra round after max_iters (python reference rule) */
-  int32_t reserved[6];
+  int32_t light_heavy;      /* delta: relax light edges (w <= delta) per sub-phase and heavy
+                               edges once per settled vertex (default 1) */
+  int32_t trace;            /* record one b2_trace_entry per phase (b2_graph_trace) */
+  int32_t reserved[4];
 } b2_sssp_opts;
+
+typedef struct b2_trace_entry {
+  uint32_t kind;        /* 1 relax, 2 commit, 3 far split, 4 probe, 5 output; | 0x100 heavy pass */
+  uint32_t frontier;    /* frontier entries of the phase */
+  uint32_t hub_chunks;  /* 256-edge chunks of split high-degree vertices */
+  uint32_t bucket;      /* delta: bucket index; BF: round */
+  uint64_t t_ns;        /* phase end, ns after the solve's first barrier */
+} b2_trace_entry;
 
 typedef struct b2_stats {
   int32_t iterations_used;  /* BF: rounds; delta/ADDS: non-empty buckets processed */
@@ -160,6 +171,8 @@ b2_status b2_graph_destroy(b2_graph g);
 b2_status b2_graph_info_get(b2_graph g, b2_graph_info* info);
 /* Near-Far delta = scale * mean(w > 0) / mean degree (>= 1 for uint32). */
 b2_status b2_delta_heuristic(b2_graph g, double scale, double* delta_out);
+/* Phase trace of the last solve on g that ran with opts.trace = 1. */
+b2_status b2_graph_trace(b2_graph g, b2_trace_entry* entries, int32_t capacity, int32_t* count);
 
 /* ---- SSSP -------------------------------------------------------------
  * d_dist: n words of the graph's weight type (uint32: 0xFFFFFFFF = unreachable;
@@ -192,6 +205,11 @@ b2_status b2_minplus_gemm_i32(const int32_t* dA, const int32_t* dB, int32_t* dC,
  * nothing.  *squarings_out = products computed. */
 b2_status b2_apsp_f32(float* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
 b2_status b2_apsp_i32(int32_t* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
+/* Sustained (min,+) pairs per second of this GPU's CUDA cores, measured by a
+ * register-only kernel of the same instruction mix as the GEMM inner loop
+ * (int32: DPX add-min; fp32: FADD + three-input min).  The roofline
+ * denominator for the min-plus GEMM.  Synchronous, current device. */
+b2_status b2_minplus_calibrate(int32_t is_float, double* pairs_per_second);
 
 /* CSR x CSR min-plus.  Outputs are cudaMalloc'd by the callee and owned by
  * the caller (cudaFree).  Absent = +inf; explicit +inf / NaN entries and

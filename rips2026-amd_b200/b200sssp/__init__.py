@@ -222,6 +222,20 @@ class Graph:
                  C.c_void_p(_stream_ptr(stream)), C.byref(st)), f"sssp[{method}]")
         return dist, pr, st.as_dict()
 
+    def trace(self) -> list[dict]:
+        """Per-phase trace of the last solve run with trace=1."""
+        cap = 4096
+        buf = (_lib.TraceEntry * cap)()
+        n = C.c_int32()
+        check(lib().b2_graph_trace(self._h, C.cast(buf, C.c_void_p), cap, C.byref(n)), "graph_trace")
+        kinds = {1: "relax", 2: "commit", 3: "split", 4: "probe", 5: "output"}
+        out = []
+        for e in buf[: n.value]:
+            out.append({"kind": kinds.get(e.kind & 0xff, str(e.kind)) + ("-heavy" if e.kind & 0x100 else ""),
+                        "frontier": e.frontier, "hub_chunks": e.hub_chunks, "bucket": e.bucket,
+                        "t_us": e.t_ns / 1e3})
+        return out
+
     def close(self) -> None:
         if self._h:
             lib().b2_graph_destroy(self._h)

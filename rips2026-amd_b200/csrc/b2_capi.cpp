@@ -41,6 +41,8 @@ extern "C" void b2_sssp_opts_default(b2_sssp_opts* o) {
   o->timeout_ms = 20000.0;
   o->collect_reach = 0;
   o->detect_negative_cycle = 0;
+  o->light_heavy = 1;
+  o->trace = 0;
 }
 
 extern "C" b2_status b2_device_free(void* p) {

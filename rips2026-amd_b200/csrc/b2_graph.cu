@@ -133,6 +133,20 @@ __global__ void k_max_degree(int64_t n, const uint64_t* rowptr, uint32_t* out) {
   atomicMax(out, mx);
 }
 
+__global__ void k_unpack(int64_t m, const uint2* e, uint32_t* key, uint32_t* dst) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    const uint2 x = e[i];
+    dst[i] = x.x;
+    key[i] = x.y;
+  }
+}
+__global__ void k_pack(int64_t m, const uint32_t* key, const uint32_t* dst, uint2* e) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+    e[i] = make_uint2(dst[i], key[i]);
+}
+
 int grid_for(int64_t items, int threads) {
   int64_t b = (items + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -180,6 +194,43 @@ b2_status finish_stats(b2_graph g, cudaStream_t st) {
   return B2_SUCCESS;
 }
 
+// Order every adjacency list by weight (stable: equal weights keep their
+// order), so the edges with weight <= delta are a prefix of each row and a
+// light pass reads exactly them.  Stable segmented radix sort, keys = weight.
+b2_status sort_rows_by_weight(b2_graph g, cudaStream_t st) {
+  const int64_t m = g->m;
+  if (m < 2) return B2_SUCCESS;
+  if (m > 0x7fffffffLL) return B2_SUCCESS;   // segmented sort item count is int; rows stay unsorted
+  DevBuf<uint32_t> k0, k1, v0, v1;
+  DevBuf<unsigned char> tmp;
+  B2_CUDA_TRY(k0.alloc((size_t)m));
+  B2_CUDA_TRY(k1.alloc((size_t)m));
+  B2_CUDA_TRY(v0.alloc((size_t)m));
+  B2_CUDA_TRY(v1.alloc((size_t)m));
+  k_unpack<<<grid_for(m, 256), 256, 0, st>>>(m, g->edges, k0.p, v0.p);
+  B2_CUDA_TRY(cudaGetLastError());
+  size_t tb = 0;
+  const int nseg = (int)g->n;
+  if (g->weight_type == B2_W_F32) {
+    B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb, (const float*)k0.p, (float*)k1.p, v0.p, v1.p,
+                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+    B2_CUDA_TRY(tmp.alloc(tb));
+    B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(tmp.p, tb, (const float*)k0.p, (float*)k1.p, v0.p, v1.p,
+                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+  } else {
+    B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb, (const uint32_t*)k0.p, k1.p, v0.p, v1.p,
+                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+    B2_CUDA_TRY(tmp.alloc(tb));
+    B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(tmp.p, tb, (const uint32_t*)k0.p, k1.p, v0.p, v1.p,
+                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+  }
+  k_pack<<<grid_for(m, 256), 256, 0, st>>>(m, k1.p, v1.p, g->edges);
+  B2_CUDA_TRY(cudaGetLastError());
+  B2_CUDA_TRY(cudaStreamSynchronize(st));
+  g->rows_sorted = true;
+  return B2_SUCCESS;
+}
+
 }  // namespace
 
 b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowptr, const uint2* edges,
@@ -195,7 +246,8 @@ b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowpt
   cudaMemcpy(g->rowptr, rowptr, (size_t)(n + 1) * sizeof(uint64_t), cudaMemcpyDeviceToDevice);
   if (m) cudaMemcpy(g->edges, edges, (size_t)m * sizeof(uint2), cudaMemcpyDeviceToDevice);
   g->graph_bytes = (size_t)(n + 1) * 8 + (size_t)m * 8;
-  b2_status s = finish_stats(g, 0);
+  b2_status s = sort_rows_by_weight(g, 0);
+  if (s == B2_SUCCESS) s = finish_stats(g, 0);
   if (s != B2_SUCCESS) { b2_graph_destroy(g); return s; }
   *out = g;
   return B2_SUCCESS;
@@ -208,6 +260,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   // (Re)allocate.
   auto fr = [](void* p) { if (p) cudaFree(p); };
   fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
+  fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
   fr(w.ctl);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   w = Workspace();
@@ -226,12 +279,16 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   if (e == cudaSuccess) e = al((void**)&w.pstamp, n * 4);
   if (e == cudaSuccess) e = al((void**)&w.bstamp, n * 4);
   if (e == cudaSuccess) e = al((void**)&w.farflag, n * 4);
-  if (e == cudaSuccess) e = al((void**)&w.queues, (4 + (size_t)kRing) * n * 4);
+  if (e == cudaSuccess) e = al((void**)&w.hstamp, n * 4);
+  if (e == cudaSuccess) e = al((void**)&w.lightcnt, n * 4);
+  if (e == cudaSuccess) e = al((void**)&w.trace, kTraceCap * sizeof(TraceEntry));
+  if (e == cudaSuccess) e = al((void**)&w.queues, (5 + (size_t)kRing) * n * 4);
   if (e == cudaSuccess) e = al((void**)&w.hubs, 2 * w.hub_cap * sizeof(HubEntry));
   if (e == cudaSuccess) e = al((void**)&w.ctl, sizeof(Control));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&w.h_ctl, sizeof(Control));
   if (e != cudaSuccess) {
     fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
+    fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
     fr(w.ctl);
     if (w.h_ctl) cudaFreeHost(w.h_ctl);
     w = Workspace();
@@ -239,6 +296,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   }
   // Stamps start at zero; phase ids handed out by solves start at 1.
   cudaMemset(w.pstamp, 0, n * 4);
+  cudaMemset(w.hstamp, 0, n * 4);
   w.phase_epoch = 1;
   w.bytes = bytes;
   return B2_SUCCESS;
@@ -337,7 +395,8 @@ extern "C" b2_status b2_graph_create(const b2_csr* csr, b2_stream stream, b2_gra
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   }
   if (e != cudaSuccess) { b2_graph_destroy(g); return from_cuda(e); }
-  b2_status s = finish_stats(g, st);
+  b2_status s = sort_rows_by_weight(g, st);
+  if (s == B2_SUCCESS) s = finish_stats(g, st);
   if (s != B2_SUCCESS) { b2_graph_destroy(g); return s; }
   *out = g;
   return B2_SUCCESS;
@@ -349,6 +408,7 @@ extern "C" b2_status b2_graph_destroy(b2_graph g) {
   auto fr = [](void* p) { if (p) cudaFree(p); };
   fr(g->rowptr); fr(g->edges); fr(g->in_rowptr32);
   fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
+  fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
   fr(w.ctl);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   delete g;

@@ -55,7 +55,21 @@ struct PhaseRec {
   uint32_t win;         // window base bucket (delta)
   uint32_t far_sel;     // far pile being appended to (delta)
   uint32_t iter;        // BF iteration being executed
+  uint32_t heavy;       // 1: relax the heavy suffix (w > delta) of each frontier vertex
+  uint32_t hround;      // stamp of the current heavy round (members dedup)
+  uint32_t aux;         // BF: round role (0 normal, 2 commit-before-probe, 1 probe); FINAL: source buffer
+  uint32_t pad;
 };
+
+// One entry per executed phase when tracing is on (manager-written).
+struct TraceEntry {
+  uint32_t kind;        // PhaseKind | heavy << 8
+  uint32_t fcount;      // frontier entries
+  uint32_t hub_chunks;  // hub chunks consumed
+  uint32_t cur;         // bucket (delta) or round (BF)
+  unsigned long long t_ns;  // end of the phase, ns since the first barrier
+};
+constexpr uint32_t kTraceCap = 4096;
 
 enum PhaseKind : uint32_t {
   kPhaseInit = 0,
@@ -72,7 +86,8 @@ enum QueueId : uint32_t {
   kQNear1 = 1,
   kQFar0 = 2,
   kQFar1 = 3,
-  kQSlot0 = 4,   // kQSlot0 + s, s < kRing
+  kQMembers = 4,  // vertices settled in the current heavy round
+  kQSlot0 = 5,    // kQSlot0 + s, s < kRing
   kQNone = 0xFFFFFFFFu,
 };
 
@@ -92,6 +107,8 @@ struct Control {
   unsigned long long hub_packed[2];  // (entries << 36) | chunks
   uint32_t bucket_valid;   // a valid vertex was processed in the current bucket
   uint32_t probe_valid;    // PROBE phase result
+  uint32_t members_count;  // entries in the heavy-round member list
+  uint32_t trace_n;
   // results
   uint32_t iterations;
   uint32_t converged;
@@ -114,7 +131,13 @@ struct Workspace {
   uint32_t* pstamp = nullptr; // near-queue dedup stamps
   uint32_t* bstamp = nullptr; // min bucket pushed (delta)
   uint32_t* farflag = nullptr;
-  uint32_t* queues = nullptr; // (4 + kRing) * n ids
+  uint32_t* hstamp = nullptr; // heavy-round member stamps
+  uint32_t* lightcnt = nullptr; // per vertex: edges with weight <= delta (sorted prefix)
+  uint32_t light_key_valid = 0;
+  uint32_t light_key = 0;     // delta (uint32) or its float bits the counts were built for
+  TraceEntry* trace = nullptr;
+  uint32_t trace_n = 0;       // entries recorded by the last traced solve
+  uint32_t* queues = nullptr; // (5 + kRing) * n ids
   HubEntry* hubs = nullptr;   // 2 * hub_cap
   size_t hub_cap = 0;
   Control* ctl = nullptr;
@@ -137,6 +160,7 @@ struct b2_graph_s {
   double mean_degree = 0.0;
   int32_t max_degree = 0;
   bool has_negative = false;
+  bool rows_sorted = false;     // each adjacency list ordered by weight
   size_t graph_bytes = 0;
   b2::Workspace ws;
   std::mutex mu;   // one solve at a time per handle

@@ -9,19 +9,28 @@
 // (delta_stepping_hip_CSR.cpp:701-780: several D2H syncs per bucket;
 // bf_hip_CSR.cpp:58-95: one sync per iteration).
 //
-// Relaxation (per phase): each warp takes 32 frontier vertices, scans their
-// out-degrees and walks the concatenated edge lists 32 edges at a time, so
-// lanes read consecutive (dst, w) pairs; the owner of an edge slot is found by
-// a 5-step shuffle binary search over the warp's inclusive degree scan.
-// Vertices with out-degree >= hub_degree are split into 256-edge chunks that
-// any warp of the grid processes in the next phase.  A relaxation is a
-// load (filter) plus one hardware atomicMin on the 32-bit key or the packed
-// 64-bit key|pred word; pushes are warp-aggregated.
+// Relaxation (per phase): each warp takes 32 frontier vertices, drops the
+// ones with nothing to relax, scans the rest's edge counts and walks the
+// concatenated edge ranges 128 slots per step (4 per lane), so lanes read
+// consecutive (dst, w) pairs.  The owner of an edge slot comes from one
+// warp-OR of "range starts here" bits per 32-slot window plus a popcount, and
+// all four edges' loads are issued before their atomics.  Vertices with
+// at least hub_degree edges in the phase's range are split into 256-edge
+// chunks that any warp takes in the next phase.  A relaxation is an L2 load
+// (filter) plus one hardware atomicMin on the 32-bit key or the packed 64-bit
+// key|pred word; pushes are warp-aggregated.
 //
-// Delta-stepping bucket structure (replaces the reference's host-driven
-// current/pending/heavy queues, delta_stepping_hip_CSR.cpp:367-529):
-//   * near queues (2, ping-pong): vertices whose new distance falls in the
-//     current bucket; deduplicated per phase with a stamp word;
+// Delta-stepping (replaces the reference's host-driven current / pending /
+// heavy queues, delta_stepping_hip_CSR.cpp:367-529):
+//   * adjacency lists are sorted by weight when the graph is built, so the
+//     light edges (w <= delta) of a vertex are a prefix of its row; the
+//     prefix length per vertex is computed once per delta (k_light_count);
+//   * light sub-phases relax only the prefix; every vertex settled in them is
+//     appended once (stamp) to a member list, and a heavy phase relaxes the
+//     suffix of each member once with its final label, like the reference's
+//     heavy queue (relax_heavy_edges_kernel, :425-459);
+//   * near queues (2, ping-pong) hold same-bucket improvements, deduplicated
+//     per phase by a stamp word;
 //   * a window of kRing buckets [win, win + kRing), one queue each,
 //     deduplicated by a per-vertex "smallest bucket pushed" word;
 //   * a far pile for buckets past the window, one entry per vertex (flag),
@@ -34,6 +43,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "b2_common.cuh"
 #include "b2_internal.hpp"
@@ -42,21 +52,25 @@ namespace b2 {
 
 enum Mode : int { kModeBF = 0, kModeDelta = 1 };
 constexpr int kThreads = 512;
+constexpr int kUnroll = 4;   // edge slots per lane per step
 
 struct Params {
   uint32_t n;
   uint32_t source;
   const uint64_t* __restrict__ rowptr;
   const uint2* __restrict__ edges;
+  const uint32_t* __restrict__ lightcnt;   // null: relax whole rows in every sub-phase
   void* dist;        // labels receiving atomicMin (BF: round k+1 values)
   void* dist_cur;    // BF: labels of round k (read side)
   uint32_t* pstamp;
   uint32_t* bstamp;
   uint32_t* farflag;
+  uint32_t* hstamp;
   uint32_t* queues;
   HubEntry* hubs;
   uint32_t hub_cap;
   Control* ctl;
+  TraceEntry* trace;
   uint32_t delta_u;
   float inv_delta;
   uint32_t hub_degree;
@@ -130,32 +144,37 @@ struct Tally {
   unsigned long long edges = 0, impr = 0, pushes = 0;
 };
 
-// ---------------------------------------------------------------------------
-// Relax one edge slot per lane and route improvements.  Must be called by all
-// 32 lanes of the warp (act = false lanes only take part in the aggregation).
-template <class W, bool PRED, int MODE>
-__device__ __forceinline__ void relax_route(const Params& P, const PhaseRec& R, bool act, uint32_t u,
-                                            uint32_t du, uint2 ed, Tally& t) {
-  using L = Label<PRED>;
-  typename L::T* lab = (typename L::T*)P.dist;
-  bool improved = false;
-  uint32_t v = 0, cand = kInfKey;
-  if (act) {
-    ++t.edges;
-    v = ed.x;
-    cand = W::extend(du, ed.y);
-    if (cand != kInfKey) {
-      const typename L::T cw = L::make(cand, u);
-      const typename L::T cur = ldcg(lab + v);
-      if (cw < cur) {
-        const typename L::T old = atomicMin(lab + v, cw);
-        improved = cand < L::key(old);
-        // (PRED: a smaller predecessor at an equal distance updates the word
-        //  but does not re-expand the vertex.)
-      }
-    }
+__device__ __forceinline__ uint32_t lanemask_le() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
+  return m;
+}
+
+// Position of the (k+1)-th set bit of `mask` (k < popc(mask)); pure register
+// arithmetic, 5 halving steps.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t mask, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t step = 16; step >= 1; step >>= 1) {
+    const uint32_t lowcnt = __popc(mask & ((1u << (pos + step)) - 1u));   // bits below pos+step
+    if (lowcnt <= k) pos += step;
   }
-  if (improved) ++t.impr;
+  return pos;
+}
+
+__device__ __forceinline__ unsigned long long shfl64(unsigned long long x, uint32_t src) {
+  const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)x, src);
+  const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(x >> 32), src);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+// ---------------------------------------------------------------------------
+// Route one improvement per lane into the right worklist.  Warp-collective:
+// all 32 lanes call it with `improved` possibly false.
+template <class W, int MODE>
+__device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool improved, uint32_t v,
+                                      uint32_t cand, Tally& t) {
+  if (!__any_sync(0xffffffffu, improved)) return;
   Control* c = P.ctl;
   if (MODE == kModeBF) {
     const bool want = improved && atomicExch(&P.pstamp[v], R.stamp) != R.stamp;
@@ -167,7 +186,6 @@ __device__ __forceinline__ void relax_route(const Params& P, const PhaseRec& R, 
     }
     return;
   }
-  // delta: route by bucket
   uint32_t b = 0;
   int cls = 0;  // 1 near, 2 window slot, 3 far
   if (improved) {
@@ -176,8 +194,7 @@ __device__ __forceinline__ void relax_route(const Params& P, const PhaseRec& R, 
     else if (b < R.win + (uint32_t)kRing) cls = 2;
     else cls = 3;
   }
-  // near
-  {
+  if (__any_sync(0xffffffffu, cls == 1)) {
     const bool want = (cls == 1) && atomicExch(&P.pstamp[v], R.stamp) != R.stamp;
     const uint32_t pos = warp_append(&c->near_count[R.push_q & 1], want);
     if (want) {
@@ -186,7 +203,6 @@ __device__ __forceinline__ void relax_route(const Params& P, const PhaseRec& R, 
       ++t.pushes;
     }
   }
-  // window slot
   if (__any_sync(0xffffffffu, cls == 2)) {
     const bool want = (cls == 2) && atomicMin(&P.bstamp[v], b) > b;
     if (want) {
@@ -202,7 +218,6 @@ __device__ __forceinline__ void relax_route(const Params& P, const PhaseRec& R, 
       ++t.pushes;
     }
   }
-  // far pile
   if (__any_sync(0xffffffffu, cls == 3)) {
     bool want = false;
     uint32_t bmin = 0xFFFFFFFFu;
@@ -221,11 +236,62 @@ __device__ __forceinline__ void relax_route(const Params& P, const PhaseRec& R, 
   }
 }
 
+// Relax kUnroll edge slots per lane: loads first, then atomics, then routing.
+template <class W, bool PRED, int MODE>
+__device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, const bool (&act)[kUnroll],
+                                            const uint32_t (&src)[kUnroll], const uint32_t (&dsrc)[kUnroll],
+                                            const uint2 (&ed)[kUnroll], Tally& t) {
+  using L = Label<PRED>;
+  typename L::T* lab = (typename L::T*)P.dist;
+  uint32_t cand[kUnroll];
+  typename L::T cur[kUnroll];
+  bool imp[kUnroll];
+#pragma unroll
+  for (int q = 0; q < kUnroll; ++q) {
+    cand[q] = act[q] ? W::extend(dsrc[q], ed[q].y) : kInfKey;
+    cur[q] = (cand[q] != kInfKey) ? ldcg(lab + ed[q].x) : L::kInf;
+  }
+#pragma unroll
+  for (int q = 0; q < kUnroll; ++q) {
+    imp[q] = false;
+    if (cand[q] != kInfKey) {
+      const typename L::T cw = L::make(cand[q], src[q]);
+      if (cw < cur[q]) {
+        const typename L::T old = atomicMin(lab + ed[q].x, cw);
+        // (PRED: a smaller predecessor at an equal distance updates the word
+        //  but does not re-expand the vertex.)
+        imp[q] = cand[q] < L::key(old);
+      }
+    }
+    t.edges += act[q] ? 1 : 0;
+    t.impr += imp[q] ? 1 : 0;
+  }
+#pragma unroll
+  for (int q = 0; q < kUnroll; ++q) route<W, MODE>(P, R, imp[q], ed[q].x, cand[q], t);
+}
+
 template <class W, bool PRED, int MODE>
 __device__ __forceinline__ uint32_t src_key(const Params& P, uint32_t v) {
   using L = Label<PRED>;
   const typename L::T* lab = (const typename L::T*)(MODE == kModeBF ? P.dist_cur : P.dist);
   return L::key(ldcg(lab + v));
+}
+
+// Edge range of v relaxed by this phase: the light prefix, the heavy suffix,
+// or the whole row.
+__device__ __forceinline__ void phase_range(const Params& P, const PhaseRec& R, uint32_t v, uint64_t& lo,
+                                            uint64_t& hi, bool& has_heavy) {
+  const uint64_t b = __ldg(&P.rowptr[v]);
+  const uint64_t e = __ldg(&P.rowptr[v + 1]);
+  has_heavy = false;
+  if (P.lightcnt) {
+    const uint64_t l = b + __ldg(&P.lightcnt[v]);
+    if (R.heavy) { lo = l; hi = e; }
+    else { lo = b; hi = l; has_heavy = e > l; }
+  } else {
+    lo = b;
+    hi = e;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -242,8 +308,7 @@ __device__ void process_hubs(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t c1 = min(total, c0 + per);
   if (c0 >= c1) return;
   const HubEntry* H = P.hubs + (size_t)(R.hub_in & 1) * P.hub_cap;
-  // last entry with base <= c0
-  uint32_t lo = 0, hi = cnt - 1;
+  uint32_t lo = 0, hi = cnt - 1;   // last entry with base <= c0
   while (lo < hi) {
     const uint32_t mid = (lo + hi + 1) >> 1;
     if (ldcg(&H[mid].base) <= c0) lo = mid; else hi = mid - 1;
@@ -255,18 +320,26 @@ __device__ void process_hubs(const Params& P, const PhaseRec& R, Tally& t) {
     const uint32_t du = src_key<W, PRED, MODE>(P, v);
     bool valid = du != kInfKey;
     if (MODE == kModeDelta) valid = valid && bucket_of<W>(P, du) == R.cur;
-    const uint64_t beg = __ldg(&P.rowptr[v]);
-    const uint64_t end = __ldg(&P.rowptr[v + 1]);
+    uint64_t rlo, rhi;
+    bool hh;
+    phase_range(P, R, v, rlo, rhi, hh);
     for (; c0 < c1 && c0 < next; ++c0) {
       if (!valid) continue;
-      const uint64_t e0 = beg + (uint64_t)(c0 - hb) * kHubChunk;
-      const uint64_t e1 = min(end, e0 + kHubChunk);
-      for (uint64_t eb = e0; eb < e1; eb += 32) {
-        const uint64_t e = eb + lane;
-        const bool act = e < e1;
-        uint2 ed = make_uint2(0, 0);
-        if (act) ed = __ldg(&P.edges[e]);
-        relax_route<W, PRED, MODE>(P, R, act, v, du, ed, t);
+      const uint64_t e0 = rlo + (uint64_t)(c0 - hb) * kHubChunk;
+      const uint64_t e1 = min(rhi, e0 + kHubChunk);
+      for (uint64_t eb = e0; eb < e1; eb += 32 * kUnroll) {
+        bool act[kUnroll];
+        uint32_t src[kUnroll], dsrc[kUnroll];
+        uint2 ed[kUnroll];
+#pragma unroll
+        for (int q = 0; q < kUnroll; ++q) {
+          const uint64_t e = eb + 32 * q + lane;
+          act[q] = e < e1;
+          src[q] = v;
+          dsrc[q] = du;
+          ed[q] = act[q] ? __ldg(&P.edges[e]) : make_uint2(0, 0);
+        }
+        relax_batch<W, PRED, MODE>(P, R, act, src, dsrc, ed, t);
       }
     }
   }
@@ -280,33 +353,38 @@ __device__ void process_frontier(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   Control* c = P.ctl;
+  const bool members = MODE == kModeDelta && P.lightcnt && !R.heavy;
   for (uint32_t base = gwarp * 32; base < cnt; base += nwarps * 32) {
     const uint32_t i = base + lane;
-    uint32_t v = 0, du = kInfKey, deg = 0;
-    uint64_t beg = 0;
-    bool valid = false;
+    uint32_t v = 0, du = kInfKey;
+    uint64_t lo = 0, hi = 0;
+    bool valid = false, has_heavy = false;
     if (i < cnt) {
       v = ldcg(F + i);
       du = src_key<W, PRED, MODE>(P, v);
       valid = du != kInfKey;
       if (MODE == kModeDelta) valid = valid && bucket_of<W>(P, du) == R.cur;
-      if (valid) {
-        beg = __ldg(&P.rowptr[v]);
-        const uint64_t d = __ldg(&P.rowptr[v + 1]) - beg;
-        deg = (uint32_t)min(d, (uint64_t)0xFFFFFFFFull);
-      }
+      if (valid) phase_range(P, R, v, lo, hi, has_heavy);
     }
     if (MODE == kModeDelta) {
-      if (__any_sync(0xffffffffu, valid) && lane == 0 && ldcg(&c->bucket_valid) == 0)
-        c->bucket_valid = 1;
+      if (__any_sync(0xffffffffu, valid) && lane == 0 && ldcg(&c->bucket_valid) == 0) c->bucket_valid = 1;
+      if (members) {
+        // settled in this light round: its heavy suffix is relaxed once by the heavy phase
+        const bool want = valid && has_heavy && atomicExch(&P.hstamp[v], R.hround) != R.hround;
+        const uint32_t pos = warp_append(&c->members_count, want);
+        if (want) {
+          if (pos < P.n) queue_ptr(P, kQMembers)[pos] = v;
+          else set_error(P, kErrQueueOverflow, 14);
+        }
+      }
     }
-    // hubs -> chunk list for the next phase
-    const bool hub = valid && deg >= P.hub_degree;
+    uint32_t deg = valid ? (uint32_t)min(hi - lo, (uint64_t)0xFFFFFFFFull) : 0u;
+    // high-degree ranges -> chunk list for the next phase
+    const bool hub = deg >= P.hub_degree;
     if (__any_sync(0xffffffffu, hub)) {
       if (hub) {
         const unsigned long long nch = (deg + kHubChunk - 1) / kHubChunk;
-        const unsigned long long old =
-            atomicAdd(&c->hub_packed[R.hub_out & 1], (1ull << 36) | nch);
+        const unsigned long long old = atomicAdd(&c->hub_packed[R.hub_out & 1], (1ull << 36) | nch);
         const uint32_t pos = (uint32_t)(old >> 36);
         const uint32_t cb = (uint32_t)(old & ((1ull << 36) - 1));
         if (pos < P.hub_cap) {
@@ -319,31 +397,42 @@ __device__ void process_frontier(const Params& P, const PhaseRec& R, Tally& t) {
         deg = 0;
       }
     }
-    const uint32_t incl = warp_incl_scan(deg);
+    // compact the lanes that have edges to relax
+    const uint32_t nz = __ballot_sync(0xffffffffu, deg > 0);
+    const uint32_t k = __popc(nz);
+    if (k == 0) continue;
+    const bool has = lane < k;
+    const uint32_t sl = nth_set_bit(nz, has ? lane : 0u);
+    const uint32_t cv = __shfl_sync(0xffffffffu, v, sl);
+    const uint32_t cdu = __shfl_sync(0xffffffffu, du, sl);
+    const uint32_t sdeg = __shfl_sync(0xffffffffu, deg, sl);
+    const uint32_t cdeg = has ? sdeg : 0u;
+    const unsigned long long clo = shfl64(lo, sl);
+    const uint32_t incl = warp_incl_scan(cdeg);
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    const uint32_t excl = incl - deg;
-    for (uint32_t eb = 0; eb < total; eb += 32) {
-      const uint32_t e = eb + lane;
-      const bool act = e < total;
-      // owner = number of lanes whose inclusive scan is <= e
-      uint32_t j = 0;
+    const uint32_t excl = incl - cdeg;
+    const unsigned long long ebase = clo - excl;   // edge index of slot p owned here = ebase + p
+    uint32_t started = 0;                           // ranges that start before the window
+    for (uint32_t eb = 0; eb < total; eb += 32 * kUnroll) {
+      bool act[kUnroll];
+      uint32_t src[kUnroll], dsrc[kUnroll];
+      uint2 ed[kUnroll];
 #pragma unroll
-      for (uint32_t step = 16; step >= 1; step >>= 1) {
-        const uint32_t probe = __shfl_sync(0xffffffffu, incl, j + step - 1);
-        if (probe <= e) j += step;
+      for (int q = 0; q < kUnroll; ++q) {
+        const uint32_t w0 = eb + 32 * q;
+        const uint32_t bit = (has && excl >= w0 && excl < w0 + 32) ? (1u << (excl - w0)) : 0u;
+        const uint32_t starts = __reduce_or_sync(0xffffffffu, bit);
+        uint32_t own = started + __popc(starts & lanemask_le()) - 1;
+        started += __popc(starts);
+        own = min(own, 31u);
+        const uint32_t p = w0 + lane;
+        act[q] = p < total;
+        src[q] = __shfl_sync(0xffffffffu, cv, own);
+        dsrc[q] = __shfl_sync(0xffffffffu, cdu, own);
+        const unsigned long long e = shfl64(ebase, own) + p;
+        ed[q] = act[q] ? __ldg(&P.edges[e]) : make_uint2(0, 0);
       }
-      j = min(j, 31u);
-      const uint32_t o_excl = __shfl_sync(0xffffffffu, excl, j);
-      const uint32_t o_lo = __shfl_sync(0xffffffffu, (uint32_t)beg, j);
-      const uint32_t o_hi = __shfl_sync(0xffffffffu, (uint32_t)(beg >> 32), j);
-      const uint32_t o_v = __shfl_sync(0xffffffffu, v, j);
-      const uint32_t o_du = __shfl_sync(0xffffffffu, du, j);
-      uint2 ed = make_uint2(0, 0);
-      if (act) {
-        const uint64_t ebeg = ((uint64_t)o_hi << 32) | o_lo;
-        ed = __ldg(&P.edges[ebeg + (e - o_excl)]);
-      }
-      relax_route<W, PRED, MODE>(P, R, act, o_v, o_du, ed, t);
+      relax_batch<W, PRED, MODE>(P, R, act, src, dsrc, ed, t);
     }
   }
 }
@@ -353,6 +442,21 @@ __device__ void process_frontier(const Params& P, const PhaseRec& R, Tally& t) {
 __device__ __forceinline__ uint32_t vld(const uint32_t* p) { return *(const volatile uint32_t*)p; }
 __device__ __forceinline__ unsigned long long vld64(const unsigned long long* p) {
   return *(const volatile unsigned long long*)p;
+}
+
+__device__ __forceinline__ void trace_phase(const Params& P, const PhaseRec& r, uint32_t tag) {
+  if (!P.trace) return;
+  Control* c = P.ctl;
+  const uint32_t i = vld(&c->trace_n);
+  if (i >= kTraceCap) return;
+  TraceEntry e;
+  e.kind = r.kind | (r.heavy ? 0x100u : 0u);
+  e.fcount = r.fcount;
+  e.hub_chunks = r.hub_in_chunks;
+  e.cur = tag;
+  e.t_ns = globaltimer_ns() - c->t_start;
+  P.trace[i] = e;
+  c->trace_n = i + 1;
 }
 
 template <bool PRED, int MODE>
@@ -379,11 +483,9 @@ __device__ void manager_init(const Params& P) {
   r.fcount = 1;
   r.push_q = kQNear1;
   r.stamp = P.phase_base + 1;
+  r.hround = P.phase_base + 1;
   r.hub_in = 1;
   r.hub_out = 0;
-  r.cur = 0;
-  r.win = 0;
-  r.far_sel = 0;
   r.iter = 1;
   store_rec(c, r);
 }
@@ -404,24 +506,26 @@ __device__ __forceinline__ bool over_budget(const Params& P, PhaseRec& nx) {
 
 __device__ __forceinline__ void consume_process_counters(Control* c, const PhaseRec& r) {
   if (r.fq == kQNear0 || r.fq == kQNear1) c->near_count[r.fq] = 0;
+  else if (r.fq == kQMembers) c->members_count = 0;
   else if (r.fq >= kQSlot0 && r.fq < kQSlot0 + kRing) c->slot_count[r.fq - kQSlot0] = 0;
   if (r.hub_in_chunks) c->hub_packed[r.hub_in & 1] = 0ull;
 }
 
-// BF round bookkeeping.  PhaseRec.far_sel is reused as the round's role:
-// 0 = ordinary round, 2 = ordinary round whose commit precedes the
-// negative-cycle probe, 1 = the probe round (python reference: one extra
-// relaxation after max_iters, minplus_bellman_ford.py:92-99).
+// BF round bookkeeping.  PhaseRec.aux is the round's role: 0 ordinary round,
+// 2 ordinary round whose commit precedes the negative-cycle probe, 1 the probe
+// round (python reference: one extra relaxation after max_iters,
+// minplus_bellman_ford.py:92-99).  At FINAL, aux = 1 means "output the
+// committed round".
 __device__ void manager_bf(const Params& P) {
   Control* c = P.ctl;
   const PhaseRec r = load_rec(c);
+  trace_phase(P, r, r.iter);
   PhaseRec nx = r;
   nx.phase = r.phase + 1;
   c->phases = vld(&c->phases) + 1;
   if (r.kind == kPhaseFinal) { nx.kind = kPhaseDone; store_rec(c, nx); return; }
   if (over_budget(P, nx)) return;
   if (r.kind == kPhaseCommit) {
-    // frontier F_k is committed; relax it next.
     nx.kind = kPhaseProcess;
     nx.fq = r.fq;
     nx.fcount = r.fcount;
@@ -431,16 +535,15 @@ __device__ void manager_bf(const Params& P) {
     nx.hub_in_count = 0;
     nx.hub_in_chunks = 0;
     nx.iter = r.iter + 1;
-    nx.far_sel = (r.far_sel == 2u) ? 1u : 0u;
+    nx.aux = (r.aux == 2u) ? 1u : 0u;
     store_rec(c, nx);
     return;
   }
-  // PROCESS (a relaxation round, possibly continued by a hub-only phase)
   consume_process_counters(c, r);
   const unsigned long long hp = vld64(&c->hub_packed[r.hub_out & 1]);
   const uint32_t hcnt = (uint32_t)(hp >> 36);
   const uint32_t hch = (uint32_t)(hp & ((1ull << 36) - 1));
-  if (hch > 0) {
+  if (hch > 0) {   // hub chunks of this round: same round, same push queue and stamp
     nx.kind = kPhaseProcess;
     nx.fq = kQNone;
     nx.fcount = 0;
@@ -448,16 +551,16 @@ __device__ void manager_bf(const Params& P) {
     nx.hub_in_count = hcnt;
     nx.hub_in_chunks = hch;
     nx.hub_out = r.hub_out ^ 1u;
-    store_rec(c, nx);   // same round, same push queue and stamp
+    store_rec(c, nx);
     return;
   }
   const uint32_t nn = vld(&c->near_count[r.push_q & 1]);
   const bool changed = nn > 0;
   nx.hub_in_chunks = 0;
   nx.hub_in_count = 0;
-  if (r.far_sel == 1u) {
+  if (r.aux == 1u) {
     c->negative_cycle = changed ? 1u : 0u;
-    nx.kind = kPhaseFinal;   // far_sel stays 1: output the committed round
+    nx.kind = kPhaseFinal;   // aux stays 1: output the committed round
     store_rec(c, nx);
     return;
   }
@@ -466,26 +569,27 @@ __device__ void manager_bf(const Params& P) {
     c->converged = 1;
     c->first_unchanged = r.iter;
     nx.kind = kPhaseFinal;
-    nx.far_sel = 0u;
+    nx.aux = 0u;
     store_rec(c, nx);
     return;
   }
   if (r.iter >= P.max_iters && !P.detect_negcycle) {
     nx.kind = kPhaseFinal;
-    nx.far_sel = 0u;
+    nx.aux = 0u;
     store_rec(c, nx);
     return;
   }
   nx.kind = kPhaseCommit;
   nx.fq = r.push_q;
   nx.fcount = nn;
-  nx.far_sel = (r.iter >= P.max_iters) ? 2u : 0u;
+  nx.aux = (r.iter >= P.max_iters) ? 2u : 0u;
   store_rec(c, nx);
 }
 
 __device__ void manager_delta(const Params& P) {
   Control* c = P.ctl;
   const PhaseRec r = load_rec(c);
+  trace_phase(P, r, r.cur);
   PhaseRec nx = r;
   nx.phase = r.phase + 1;
   nx.stamp = P.phase_base + nx.phase;
@@ -507,23 +611,49 @@ __device__ void manager_delta(const Params& P) {
     c->far_min = vld(&c->far_min_next);
     c->far_min_next = 0xFFFFFFFFu;
     from_slot = 0;
-  } else {  // PROCESS
+  } else {  // PROCESS (light or heavy)
     consume_process_counters(c, r);
     const unsigned long long hp = vld64(&c->hub_packed[r.hub_out & 1]);
     const uint32_t hcnt = (uint32_t)(hp >> 36);
     const uint32_t hch = (uint32_t)(hp & ((1ull << 36) - 1));
     const uint32_t nn = vld(&c->near_count[r.push_q & 1]);
-    if (nn > 0 || hch > 0) {
-      nx.kind = kPhaseProcess;
-      nx.fq = nn ? r.push_q : kQNone;
-      nx.fcount = nn;
-      nx.push_q = r.push_q ^ 1u;
-      nx.hub_in = r.hub_out;
-      nx.hub_in_count = hcnt;
-      nx.hub_in_chunks = hch;
-      nx.hub_out = r.hub_out ^ 1u;
-      store_rec(c, nx);
-      return;
+    nx.hub_in = r.hub_out;
+    nx.hub_in_count = hcnt;
+    nx.hub_in_chunks = hch;
+    nx.hub_out = r.hub_out ^ 1u;
+    if (r.heavy) {
+      if (hch > 0) {             // heavy hub chunks first; near pushes keep accumulating
+        nx.fq = kQNone;
+        nx.fcount = 0;
+        nx.stamp = r.stamp;
+        store_rec(c, nx);
+        return;
+      }
+      if (nn > 0) {              // a heavy relaxation landed in this bucket: new light round
+        nx.heavy = 0;
+        nx.fq = r.push_q;
+        nx.fcount = nn;
+        nx.push_q = r.push_q ^ 1u;
+        nx.hround = P.phase_base + nx.phase;
+        store_rec(c, nx);
+        return;
+      }
+    } else {
+      if (nn > 0 || hch > 0) {
+        nx.fq = nn ? r.push_q : kQNone;
+        nx.fcount = nn;
+        nx.push_q = r.push_q ^ 1u;
+        store_rec(c, nx);
+        return;
+      }
+      const uint32_t mc = vld(&c->members_count);
+      if (mc > 0) {              // light rounds of this bucket are done: heavy pass
+        nx.heavy = 1;
+        nx.fq = kQMembers;
+        nx.fcount = mc;
+        store_rec(c, nx);
+        return;
+      }
     }
     // bucket r.cur is settled
     if (vld(&c->bucket_valid)) {
@@ -532,6 +662,7 @@ __device__ void manager_delta(const Params& P) {
     }
     if (vld(&c->iterations) >= P.max_iters) {
       nx.kind = kPhaseProbe;
+      nx.heavy = 0;
       nx.hub_in_chunks = 0;
       store_rec(c, nx);
       return;
@@ -546,6 +677,8 @@ __device__ void manager_delta(const Params& P) {
   for (int s = (int)from_slot; s < kRing; ++s) {
     if (cnts[s]) { found = s; break; }
   }
+  nx.heavy = 0;
+  nx.hround = P.phase_base + nx.phase;
   nx.far_sel = far_sel;
   nx.hub_in = r.hub_out;
   nx.hub_in_count = 0;
@@ -654,7 +787,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
       bool any = false;
       const uint32_t first = R.cur - R.win + 1;
       for (uint32_t s = first; s < (uint32_t)kRing && !any; ++s) {
-        const uint32_t cnt = ldcg(&c->slot_count[s]);
+        const uint32_t cnt = min(ldcg(&c->slot_count[s]), P.n);
         const uint32_t* F = queue_ptr(P, kQSlot0 + s);
         for (size_t i = tid; i < cnt; i += stride) {
           const uint32_t v = ldcg(F + i);
@@ -663,7 +796,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
         }
       }
       {
-        const uint32_t cnt = ldcg(&c->far_count[R.far_sel]);
+        const uint32_t cnt = min(ldcg(&c->far_count[R.far_sel]), P.n);
         const uint32_t* F = queue_ptr(P, kQFar0 + R.far_sel);
         for (size_t i = tid; i < cnt && !any; i += stride) {
           const uint32_t v = ldcg(F + i);
@@ -673,15 +806,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
       }
       if (any) c->probe_valid = 1u;
     } else if (R.kind == kPhaseFinal) {
-      // far_sel == 1 (BF probe round): the answer is the committed round.
-      const typename L::T* src =
-          (const typename L::T*)((MODE == kModeBF && R.far_sel == 1u) ? P.dist_cur : P.dist);
+      const typename L::T* srcl =
+          (const typename L::T*)((MODE == kModeBF && R.aux == 1u) ? P.dist_cur : P.dist);
       for (size_t v = tid; v < P.n; v += stride) {
-        const typename L::T wv = ldcg(src + v);
+        const typename L::T wv = ldcg(srcl + v);
         const uint32_t k = L::key(wv);
         if (W::kFloat) {
           ((float*)P.out_dist)[v] = (k == kInfKey) ? __uint_as_float(0x7f800000u) : key_to_f32(k);
-        } else if (!P.dist_is_out || (const void*)src != P.out_dist) {
+        } else if (!P.dist_is_out || (const void*)srcl != P.out_dist) {
           ((uint32_t*)P.out_dist)[v] = k;
         }
         if (PRED && P.out_pred) {
@@ -709,6 +841,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
     if (e) atomicAdd(&c->edges, e);
     if (im) atomicAdd(&c->improvements, im);
     if (pu) atomicAdd(&c->pushes, pu);
+  }
+}
+
+// Light prefix length of every row for one delta (rows sorted by weight):
+// the number of edges with weight <= delta, by binary search.
+__global__ void k_light_count(uint32_t n, const uint64_t* __restrict__ rowptr, const uint2* __restrict__ edges,
+                              int is_float, uint32_t delta_u, float delta_f, uint32_t* out) {
+  for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x) {
+    uint64_t lo = rowptr[v], hi = rowptr[v + 1];
+    const uint64_t b = lo;
+    while (lo < hi) {   // first edge with weight > delta
+      const uint64_t mid = (lo + hi) >> 1;
+      const uint32_t w = edges[mid].y;
+      const bool light = is_float ? (__uint_as_float(w) <= delta_f) : (w <= delta_u);
+      if (light) lo = mid + 1; else hi = mid;
+    }
+    out[v] = (uint32_t)min(lo - b, (uint64_t)0xFFFFFFFFull);
   }
 }
 
@@ -762,6 +911,20 @@ b2_status map_device_error(uint32_t e) {
   }
 }
 
+b2_status ensure_light_counts(b2_graph g, bool isf, uint32_t delta_u, float delta_f, cudaStream_t st) {
+  Workspace& w = g->ws;
+  uint32_t key;
+  memcpy(&key, &delta_f, 4);
+  if (!isf) key = delta_u;
+  if (w.light_key_valid && w.light_key == key) return B2_SUCCESS;
+  k_light_count<<<1184, 256, 0, st>>>((uint32_t)g->n, g->rowptr, g->edges, isf ? 1 : 0, delta_u, delta_f,
+                                      w.lightcnt);
+  B2_CUDA_TRY(cudaGetLastError());
+  w.light_key = key;
+  w.light_key_valid = 1;
+  return B2_SUCCESS;
+}
+
 b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t* d_pred,
                    const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats) {
   if (!g || !d_dist) return B2_INVALID_ARGUMENT;
@@ -785,16 +948,17 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   P.pstamp = w.pstamp;
   P.bstamp = w.bstamp;
   P.farflag = w.farflag;
+  P.hstamp = w.hstamp;
   P.queues = w.queues;
   P.hubs = w.hubs;
   P.hub_cap = (uint32_t)w.hub_cap;
   P.ctl = w.ctl;
+  P.trace = o.trace ? w.trace : nullptr;
   P.hub_degree = std::max<uint32_t>(32u, o.hub_degree ? o.hub_degree : 256u);
   P.out_dist = d_dist;
   P.out_pred = d_pred;
   P.is_float = isf ? 1u : 0u;
   P.budget_ns = (unsigned long long)(std::max(1.0, o.timeout_ms > 0 ? o.timeout_ms : 20000.0) * 1.0e6);
-  // label buffers
   if (pred) {
     P.dist = w.dist_a;
     P.dist_cur = w.dist_b;
@@ -810,14 +974,14 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     if (mi > 0x7fffffff) mi = 0x7fffffff;
     P.max_iters = (uint32_t)mi;
     P.detect_negcycle = o.detect_negative_cycle ? 1u : 0u;
-    // the zero key of the weight type is chosen in manager_init from these:
     P.inv_delta = 1.0f;
     P.delta_u = 1u;
   } else {
     delta = o.delta;
     if (!(delta > 0.0)) b2_delta_heuristic(g, o.delta_scale > 0 ? o.delta_scale : 16.0, &delta);
+    float df = 0.0f;
     if (isf) {
-      const float df = (float)delta;
+      df = (float)delta;
       if (!(df > 0.0f) || !std::isfinite(df)) return B2_INVALID_ARGUMENT;
       P.inv_delta = 1.0f / df;
       P.delta_u = 1u;
@@ -828,22 +992,28 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
       delta = (double)P.delta_u;
     }
     P.max_iters = o.max_iters < 0 ? 0xFFFFFFFFu : (uint32_t)o.max_iters;
+    if (o.light_heavy && g->rows_sorted) {
+      s = ensure_light_counts(g, isf, P.delta_u, df, st);
+      if (s != B2_SUCCESS) return s;
+      P.lightcnt = w.lightcnt;
+    }
   }
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->delta_used = delta;
   }
-  // zero iterations: only the source is reached (reference loop never runs)
+  // zero iterations: only the source is reached (the reference loop never runs)
   if (P.max_iters == 0) {
-    // labels: fill via a tiny kernel-free path
     if (isf) {
       std::vector<float> h((size_t)g->n, INFINITY);
       h[source] = 0.0f;
       B2_CUDA_TRY(cudaMemcpyAsync(d_dist, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st));
+      B2_CUDA_TRY(cudaStreamSynchronize(st));
     } else {
       std::vector<uint32_t> h((size_t)g->n, 0xFFFFFFFFu);
       h[source] = 0u;
       B2_CUDA_TRY(cudaMemcpyAsync(d_dist, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st));
+      B2_CUDA_TRY(cudaStreamSynchronize(st));
     }
     if (pred) B2_CUDA_TRY(cudaMemsetAsync(d_pred, 0xFF, (size_t)g->n * 4, st));
     B2_CUDA_TRY(cudaStreamSynchronize(st));
@@ -852,12 +1022,13 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   // phase stamps never repeat across solves on this workspace
   if (w.phase_epoch > 0xF0000000u) {
     B2_CUDA_TRY(cudaMemsetAsync(w.pstamp, 0, (size_t)g->n * 4, st));
+    B2_CUDA_TRY(cudaMemsetAsync(w.hstamp, 0, (size_t)g->n * 4, st));
     w.phase_epoch = 1;
   }
   P.phase_base = w.phase_epoch;
 
-  int grid;
-  cudaError_t e;
+  int grid = 0;
+  cudaError_t e = cudaSuccess;
   B2_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(Control), st));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -888,6 +1059,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   if (e != cudaSuccess) return from_cuda(e);
   const Control& hc = *w.h_ctl;
   w.phase_epoch += hc.rec.phase + 2;
+  w.trace_n = o.trace ? hc.trace_n : 0;
   b2_status ds = map_device_error(hc.error);
   if (stats) {
     stats->iterations_used = (int32_t)hc.iterations;
@@ -933,4 +1105,15 @@ extern "C" b2_status b2_sssp_bf(b2_graph g, uint32_t source, void* d_dist, int32
 extern "C" b2_status b2_sssp_delta(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
                                    const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats) {
   return run_sssp(g, kModeDelta, source, d_dist, d_pred, opts, (cudaStream_t)stream, stats);
+}
+
+extern "C" b2_status b2_graph_trace(b2_graph g, b2_trace_entry* entries, int32_t capacity, int32_t* count) {
+  if (!g || !count || (capacity > 0 && !entries)) return B2_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g->mu);
+  const int32_t n = (int32_t)std::min<uint32_t>(g->ws.trace_n, (uint32_t)std::max(capacity, 0));
+  *count = n;
+  if (n == 0 || !g->ws.trace) return B2_SUCCESS;
+  static_assert(sizeof(TraceEntry) == sizeof(b2_trace_entry), "trace layout");
+  B2_CUDA_TRY(cudaMemcpy(entries, g->ws.trace, (size_t)n * sizeof(TraceEntry), cudaMemcpyDeviceToHost));
+  return B2_SUCCESS;
 }

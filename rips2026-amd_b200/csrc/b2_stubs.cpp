@@ -5,12 +5,6 @@ extern "C" b2_status b2_sssp_adds(b2_graph, uint32_t, void*, int32_t*, const b2_
                                   b2_stats*) { return B2_NOT_SUPPORTED; }
 extern "C" b2_status b2_sssp_bf_dense(const float*, int32_t, uint32_t, float*, const b2_sssp_opts*,
                                       b2_stream, b2_stats*) { return B2_NOT_SUPPORTED; }
-extern "C" b2_status b2_minplus_gemm_f32(const float*, const float*, float*, int32_t, int32_t, int32_t,
-                                         int32_t, int32_t, int32_t, b2_stream) { return B2_NOT_SUPPORTED; }
-extern "C" b2_status b2_minplus_gemm_i32(const int32_t*, const int32_t*, int32_t*, int32_t, int32_t,
-                                         int32_t, int32_t, int32_t, int32_t, b2_stream) { return B2_NOT_SUPPORTED; }
-extern "C" b2_status b2_apsp_f32(float*, int32_t, b2_stream, int32_t*) { return B2_NOT_SUPPORTED; }
-extern "C" b2_status b2_apsp_i32(int32_t*, int32_t, b2_stream, int32_t*) { return B2_NOT_SUPPORTED; }
 extern "C" b2_status b2_minplus_spgemm_f32(const b2_csr*, const b2_csr*, int64_t**, int32_t**, float**,
                                            int64_t*, b2_stream) { return B2_NOT_SUPPORTED; }
 extern "C" b2_status b2_minplus_spgemm_i32(const b2_csr*, const b2_csr*, int64_t**, int32_t**, int32_t**,

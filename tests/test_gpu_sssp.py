@@ -231,3 +231,35 @@ def test_repeatable_and_large_properties(b2, orc, cuda):
     reached = ref != INF_U
     assert st1["reached"] == int(reached.sum())
     assert st1["reached_edges"] == int(np.diff(hg.rowptr)[reached].sum())
+
+
+def test_light_heavy_split_is_schedule_only(b2, orc, cuda):
+    """Relaxing light edges per sub-phase and heavy edges once per settled
+    vertex changes work, never distances or the bucket count."""
+    for hg in (b2.gen_rmat(12, 16, seed=21), b2.gen_grid(64, 64, 0.02, seed=22)):
+        for weight in ("u32", "f32"):
+            g = _graph(b2, hg, weight)
+            delta = 40.0 if weight == "u32" else 0.03
+            d1, _, s1 = g.sssp(3, method="delta", delta=delta, light_heavy=1)
+            d0, _, s0 = g.sssp(3, method="delta", delta=delta, light_heavy=0)
+            assert np.array_equal(_np(d1), _np(d0))
+            assert s1["iterations_used"] == s0["iterations_used"]
+            w = hg.weights if weight == "u32" else hg.fweights
+            ref = orc.dijkstra(hg.rowptr, hg.colind, w, 3)
+            got = _dist_u32(d1) if weight == "u32" else _np(d1)
+            assert np.array_equal(got, ref)
+            g.close()
+
+
+def test_phase_trace(b2, cuda):
+    hg = b2.gen_rmat(12, 8, seed=23)
+    g = _graph(b2, hg, "u32")
+    _, _, st = g.sssp(0, method="delta", trace=1)
+    tr = g.trace()
+    assert len(tr) == st["phases"]
+    assert tr[-1]["kind"] == "output"
+    ts = [e["t_us"] for e in tr]
+    assert ts == sorted(ts)
+    assert any(e["kind"] == "relax-heavy" for e in tr)
+    _, _, st = g.sssp(0, method="bf", trace=1)
+    assert len(g.trace()) == st["phases"]
