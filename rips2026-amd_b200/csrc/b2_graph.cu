@@ -272,7 +272,9 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
     bytes += b;
     return cudaMalloc(p, std::max<size_t>(b, 16));
   };
-  w.hub_cap = std::min<size_t>(n, (size_t)g->m / 32 + 1) + 1;
+  // chunks per phase <= sum over hub vertices of ceil(range / 256), and a hub
+  // range has >= 32 edges: at most m / 256 + m / 32 chunks.
+  w.hub_cap = std::min<size_t>((size_t)g->m / kHubChunk + (size_t)g->m / 32 + 2, 0xFFFFFFF0ull);
   cudaError_t e = cudaSuccess;
   if (e == cudaSuccess) e = al(&w.dist_a, n * word);
   if (e == cudaSuccess) e = al(&w.dist_b, n * word);

@@ -32,9 +32,10 @@ constexpr int kRing = 16;
 // chunks of this many edges that any warp of the grid may take).
 constexpr uint32_t kHubChunk = 256;
 
+// One 256-edge chunk of a high-degree vertex's phase range.
 struct HubEntry {
   uint32_t v;
-  uint32_t base;   // first global chunk index owned by v in this list
+  uint32_t chunk;  // chunk index within v's edge range of the phase
 };
 
 // Control block of one persistent solve (device memory).  The manager step
@@ -104,7 +105,8 @@ struct Control {
   uint32_t slot_count[kRing];
   uint32_t far_min;        // lower bound of buckets in the active far pile
   uint32_t far_min_next;   // exact min of the kept entries during a split
-  unsigned long long hub_packed[2];  // (entries << 36) | chunks
+  uint32_t hub_count[2];   // chunk entries in each hub list
+  uint32_t work_next;      // dynamic work counter of the running phase
   uint32_t bucket_valid;   // a valid vertex was processed in the current bucket
   uint32_t probe_valid;    // PROBE phase result
   uint32_t members_count;  // entries in the heavy-round member list
