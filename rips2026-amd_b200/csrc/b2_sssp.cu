@@ -143,7 +143,37 @@ __device__ __forceinline__ void store_rec(Control* c, const PhaseRec& r) {
 
 struct Tally {
   unsigned long long edges = 0, impr = 0, pushes = 0;
+  uint64_t keep = 0;   // L2 evict_last cache policy for label traffic
 };
+
+// Label loads and atomics carry an L2 evict_last policy: the label array is
+// read once per relaxed edge at random, so it must stay resident while the
+// edge stream (evict-first loads) flows through L2.
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint32_t ld_keep(const uint32_t* a, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.cg.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_keep(const unsigned long long* a, uint64_t pol) {
+  unsigned long long v;
+  asm volatile("ld.global.cg.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t atom_min_keep(uint32_t* a, uint32_t x, uint64_t pol) {
+  uint32_t old;
+  asm volatile("atom.global.L2::cache_hint.min.u32 %0, [%1], %2, %3;" : "=r"(old) : "l"(a), "r"(x), "l"(pol) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long atom_min_keep(unsigned long long* a, unsigned long long x, uint64_t pol) {
+  unsigned long long old;
+  asm volatile("atom.global.L2::cache_hint.min.u64 %0, [%1], %2, %3;" : "=l"(old) : "l"(a), "l"(x), "l"(pol) : "memory");
+  return old;
+}
 
 __device__ __forceinline__ uint32_t lanemask_le() {
   uint32_t m;
@@ -250,7 +280,7 @@ __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, 
 #pragma unroll
   for (int q = 0; q < kUnroll; ++q) {
     cand[q] = act[q] ? W::extend(dsrc[q], ed[q].y) : kInfKey;
-    cur[q] = (cand[q] != kInfKey) ? ldcg(lab + ed[q].x) : L::kInf;
+    cur[q] = (cand[q] != kInfKey) ? ld_keep(lab + ed[q].x, t.keep) : L::kInf;
   }
 #pragma unroll
   for (int q = 0; q < kUnroll; ++q) {
@@ -258,7 +288,7 @@ __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, 
     if (cand[q] != kInfKey) {
       const typename L::T cw = L::make(cand[q], src[q]);
       if (cw < cur[q]) {
-        const typename L::T old = atomicMin(lab + ed[q].x, cw);
+        const typename L::T old = atom_min_keep(lab + ed[q].x, cw, t.keep);
         // (PRED: a smaller predecessor at an equal distance updates the word
         //  but does not re-expand the vertex.)
         imp[q] = cand[q] < L::key(old);
@@ -422,19 +452,26 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
 // A relaxation phase: hub chunks of the previous phase, then 32-vertex
 // frontier chunks, handed out one at a time from a phase counter so no warp
 // idles while another holds a long tail.
+constexpr uint32_t kHubGrab = 4;   // hub chunks per work grab (1024 edges)
+
 template <class W, bool PRED, int MODE>
 __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t nhub = min(R.hub_in_chunks, P.hub_cap);
+  const uint32_t nhg = (nhub + kHubGrab - 1) / kHubGrab;
   const uint32_t nfc = (R.fcount + 31) / 32;
-  const uint32_t items = nhub + nfc;
+  const uint32_t items = nhg + nfc;
   Control* c = P.ctl;
   for (;;) {
     uint32_t item = 0;
     if (lane_id() == 0) item = atomicAdd(&c->work_next, 1u);
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= items) break;
-    if (item < nhub) hub_chunk<W, PRED, MODE>(P, R, item, t);
-    else frontier_chunk<W, PRED, MODE>(P, R, (item - nhub) * 32, t);
+    if (item < nhg) {
+      const uint32_t h1 = min(nhub, (item + 1) * kHubGrab);
+      for (uint32_t h = item * kHubGrab; h < h1; ++h) hub_chunk<W, PRED, MODE>(P, R, h, t);
+    } else {
+      frontier_chunk<W, PRED, MODE>(P, R, (item - nhg) * 32, t);
+    }
   }
 }
 
@@ -719,6 +756,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
   using L = Label<PRED>;
   __shared__ PhaseRec s_rec;
   Tally t;
+  t.keep = l2_keep_policy();
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   Control* c = P.ctl;
