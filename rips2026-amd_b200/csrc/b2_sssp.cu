@@ -141,9 +141,26 @@ __device__ __forceinline__ void store_rec(Control* c, const PhaseRec& r) {
   for (int i = 0; i < (int)(sizeof(PhaseRec) / 4); ++i) dst[i] = src[i];
 }
 
+// Per-warp push staging (shared memory).  Worklist insertions are collected
+// per warp and published with one global atomicAdd per flush, so the queue
+// counters (one address each) see ~1/100 of the per-push atomics; flushes
+// happen when a buffer passes half full and at the end of every phase.
+constexpr int kWarpsPerBlock = kThreads / 32;
+constexpr uint32_t kNearBuf = 256, kFarBuf = 256, kSlotBuf = 256, kMemBuf = 128;
+constexpr uint32_t kStageWords = kNearBuf + kFarBuf + 2 * kSlotBuf + kMemBuf;
+constexpr size_t kStageBytes = (size_t)kWarpsPerBlock * kStageWords * 4;
+struct WarpQ {
+  uint32_t* nearb;   // kNearBuf vertex ids
+  uint32_t* farb;    // kFarBuf
+  uint32_t* slotb;   // kSlotBuf (vertex, slot) pairs as 2 words
+  uint32_t* memb;    // kMemBuf
+  uint32_t nn = 0, nf = 0, ns = 0, nm = 0;
+};
+
 struct Tally {
   unsigned long long edges = 0, impr = 0, pushes = 0;
   uint64_t keep = 0;   // L2 evict_last cache policy for label traffic
+  WarpQ q;
 };
 
 // Label loads and atomics carry an L2 evict_last policy: the label array is
@@ -200,8 +217,98 @@ __device__ __forceinline__ unsigned long long shfl64(unsigned long long x, uint3
 }
 
 // ---------------------------------------------------------------------------
-// Route one improvement per lane into the right worklist.  Warp-collective:
-// all 32 lanes call it with `improved` possibly false.
+// Append the wanting lanes' vertices to a warp buffer (warp-collective).
+__device__ __forceinline__ void stage(uint32_t* buf, uint32_t& cnt, bool want, uint32_t v) {
+  const uint32_t b = __ballot_sync(0xffffffffu, want);
+  if (want) buf[cnt + __popc(b & ((1u << lane_id()) - 1u))] = v;
+  cnt += __popc(b);
+}
+
+// Publish a staged buffer to queue `qid` with one atomic (warp-collective).
+__device__ __forceinline__ void publish(const Params& P, uint32_t* counter, uint32_t qid, const uint32_t* buf,
+                                        uint32_t cnt, uint32_t site) {
+  if (cnt == 0) return;
+  __syncwarp();
+  uint32_t base = 0;
+  if (lane_id() == 0) base = atomicAdd(counter, cnt);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if ((uint64_t)base + cnt > P.n) {
+    if (lane_id() == 0) set_error(P, kErrQueueOverflow, site);
+    return;
+  }
+  uint32_t* dst = queue_ptr(P, qid) + base;
+  for (uint32_t i = lane_id(); i < cnt; i += 32) dst[i] = buf[i];
+  __syncwarp();
+}
+
+// Window-slot entries carry their slot: publish one slot group at a time.
+__device__ __forceinline__ void publish_slots(const Params& P, WarpQ& q) {
+  Control* c = P.ctl;
+  __syncwarp();
+  uint32_t remaining = q.ns;
+  // entries are (v, slot) pairs; process in rounds, one distinct slot per round
+  while (remaining) {
+    uint32_t s0 = q.slotb[2 * 0 + 1];
+    // lane-strided scan: count entries with slot s0
+    uint32_t mine = 0;
+    for (uint32_t i = lane_id(); i < q.ns; i += 32)
+      if (q.slotb[2 * i + 1] == s0) ++mine;
+    const uint32_t incl = warp_incl_scan(mine);
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(&c->slot_count[s0], total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((uint64_t)base + total > P.n) {
+      if (lane_id() == 0) set_error(P, kErrQueueOverflow, 12);
+      q.ns = 0;
+      return;
+    }
+    uint32_t pos = base + incl - mine;
+    uint32_t* dst = queue_ptr(P, kQSlot0 + s0);
+    for (uint32_t i = lane_id(); i < q.ns; i += 32)
+      if (q.slotb[2 * i + 1] == s0) dst[pos++] = q.slotb[2 * i];
+    __syncwarp();
+    // compact the entries of other slots to the front (single lane keeps order simple)
+    uint32_t kept = 0;
+    if (lane_id() == 0) {
+      for (uint32_t i = 0; i < q.ns; ++i)
+        if (q.slotb[2 * i + 1] != s0) {
+          q.slotb[2 * kept] = q.slotb[2 * i];
+          q.slotb[2 * kept + 1] = q.slotb[2 * i + 1];
+          ++kept;
+        }
+    }
+    kept = __shfl_sync(0xffffffffu, kept, 0);
+    __syncwarp();
+    q.ns = kept;
+    remaining = kept;
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void flush_all(const Params& P, const PhaseRec& R, WarpQ& q, bool force) {
+  Control* c = P.ctl;
+  if (q.nn && (force || q.nn > kNearBuf / 2)) {
+    publish(P, &c->near_count[R.push_q & 1], R.push_q, q.nearb, q.nn, 11);
+    q.nn = 0;
+  }
+  if (MODE == kModeBF) return;
+  if (q.nf && (force || q.nf > kFarBuf / 2)) {
+    publish(P, &c->far_count[R.far_sel], kQFar0 + R.far_sel, q.farb, q.nf, 13);
+    q.nf = 0;
+  }
+  if (q.nm && (force || q.nm > kMemBuf / 2)) {
+    publish(P, &c->members_count, kQMembers, q.memb, q.nm, 14);
+    q.nm = 0;
+  }
+  if (q.ns && (force || q.ns > kSlotBuf / 2)) publish_slots(P, q);
+  // (a relax batch adds at most 4 x 32 entries per buffer, so flushing past
+  //  half of a 256-entry buffer never overflows it)
+}
+
+// Route one improvement per lane into the right worklist (warp-collective:
+// all 32 lanes call it with `improved` possibly false).  Dedup atomics stay
+// per vertex; the insertion itself is staged in the warp's buffers.
 template <class W, int MODE>
 __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool improved, uint32_t v,
                                       uint32_t cand, Tally& t) {
@@ -209,12 +316,8 @@ __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool i
   Control* c = P.ctl;
   if (MODE == kModeBF) {
     const bool want = improved && atomicExch(&P.pstamp[v], R.stamp) != R.stamp;
-    const uint32_t pos = warp_append(&c->near_count[R.push_q & 1], want);
-    if (want) {
-      if (pos < P.n) queue_ptr(P, R.push_q)[pos] = v;
-      else set_error(P, kErrQueueOverflow, 10);
-      ++t.pushes;
-    }
+    stage(t.q.nearb, t.q.nn, want, v);
+    t.pushes += want ? 1 : 0;
     return;
   }
   uint32_t b = 0;
@@ -227,27 +330,19 @@ __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool i
   }
   if (__any_sync(0xffffffffu, cls == 1)) {
     const bool want = (cls == 1) && atomicExch(&P.pstamp[v], R.stamp) != R.stamp;
-    const uint32_t pos = warp_append(&c->near_count[R.push_q & 1], want);
-    if (want) {
-      if (pos < P.n) queue_ptr(P, R.push_q)[pos] = v;
-      else set_error(P, kErrQueueOverflow, 11);
-      ++t.pushes;
-    }
+    stage(t.q.nearb, t.q.nn, want, v);
+    t.pushes += want ? 1 : 0;
   }
   if (__any_sync(0xffffffffu, cls == 2)) {
     const bool want = (cls == 2) && atomicMin(&P.bstamp[v], b) > b;
+    const uint32_t bal = __ballot_sync(0xffffffffu, want);
     if (want) {
-      const uint32_t s = b - R.win;
-      const uint32_t grp = __match_any_sync(__activemask(), s);
-      const uint32_t leader = __ffs(grp) - 1;
-      uint32_t base = 0;
-      if (lane_id() == leader) base = atomicAdd(&c->slot_count[s], (uint32_t)__popc(grp));
-      base = __shfl_sync(grp, base, leader);
-      const uint32_t pos = base + __popc(grp & ((1u << lane_id()) - 1u));
-      if (pos < P.n) queue_ptr(P, kQSlot0 + s)[pos] = v;
-      else set_error(P, kErrQueueOverflow, 12);
-      ++t.pushes;
+      const uint32_t pos = t.q.ns + __popc(bal & ((1u << lane_id()) - 1u));
+      t.q.slotb[2 * pos] = v;
+      t.q.slotb[2 * pos + 1] = b - R.win;
     }
+    t.q.ns += __popc(bal);
+    t.pushes += want ? 1 : 0;
   }
   if (__any_sync(0xffffffffu, cls == 3)) {
     bool want = false;
@@ -258,12 +353,8 @@ __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool i
     }
     bmin = __reduce_min_sync(0xffffffffu, bmin);
     if (lane_id() == 0 && bmin != 0xFFFFFFFFu) atomicMin(&c->far_min, bmin);
-    const uint32_t pos = warp_append(&c->far_count[R.far_sel], want);
-    if (want) {
-      if (pos < P.n) queue_ptr(P, kQFar0 + R.far_sel)[pos] = v;
-      else set_error(P, kErrQueueOverflow, 13);
-      ++t.pushes;
-    }
+    stage(t.q.farb, t.q.nf, want, v);
+    t.pushes += want ? 1 : 0;
   }
 }
 
@@ -299,6 +390,7 @@ __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, 
   }
 #pragma unroll
   for (int q = 0; q < kUnroll; ++q) route<W, MODE>(P, R, imp[q], ed[q].x, cand[q], t);
+  flush_all<MODE>(P, R, t.q, false);
 }
 
 template <class W, bool PRED, int MODE>
@@ -382,10 +474,10 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
     if (members) {
       // settled in this light round: its heavy suffix is relaxed once by the heavy phase
       const bool want = valid && has_heavy && atomicExch(&P.hstamp[v], R.hround) != R.hround;
-      const uint32_t pos = warp_append(&c->members_count, want);
-      if (want) {
-        if (pos < P.n) queue_ptr(P, kQMembers)[pos] = v;
-        else set_error(P, kErrQueueOverflow, 14);
+      stage(t.q.memb, t.q.nm, want, v);
+      if (t.q.nm > kMemBuf / 2) {
+        publish(P, &c->members_count, kQMembers, t.q.memb, t.q.nm, 14);
+        t.q.nm = 0;
       }
     }
   }
@@ -452,27 +544,40 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
 // A relaxation phase: hub chunks of the previous phase, then 32-vertex
 // frontier chunks, handed out one at a time from a phase counter so no warp
 // idles while another holds a long tail.
-constexpr uint32_t kHubGrab = 4;   // hub chunks per work grab (1024 edges)
+constexpr uint32_t kHubGrab = 4;   // hub chunks per work item (1024 edges)
 
+// A relaxation phase: hub chunks of the previous phase, then 32-vertex
+// frontier chunks.  Items are first dealt round-robin to the warps (3/4 of
+// them, no atomics), the rest handed out one at a time from a phase counter
+// so no warp idles while another holds a long tail.
 template <class W, bool PRED, int MODE>
 __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t nhub = min(R.hub_in_chunks, P.hub_cap);
   const uint32_t nhg = (nhub + kHubGrab - 1) / kHubGrab;
   const uint32_t nfc = (R.fcount + 31) / 32;
   const uint32_t items = nhg + nfc;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t rounds = (items * 3 / 4) / nwarps;
+  const uint32_t nstatic = rounds * nwarps;
   Control* c = P.ctl;
-  for (;;) {
-    uint32_t item = 0;
-    if (lane_id() == 0) item = atomicAdd(&c->work_next, 1u);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= items) break;
+  auto run = [&](uint32_t item) {
     if (item < nhg) {
       const uint32_t h1 = min(nhub, (item + 1) * kHubGrab);
       for (uint32_t h = item * kHubGrab; h < h1; ++h) hub_chunk<W, PRED, MODE>(P, R, h, t);
     } else {
       frontier_chunk<W, PRED, MODE>(P, R, (item - nhg) * 32, t);
     }
+  };
+  for (uint32_t r = 0; r < rounds; ++r) run(r * nwarps + gwarp);
+  for (;;) {
+    uint32_t item = 0;
+    if (lane_id() == 0) item = atomicAdd(&c->work_next, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0) + nstatic;
+    if (item >= items) break;
+    run(item);
   }
+  flush_all<MODE>(P, R, t.q, true);
 }
 
 // ---------------------------------------------------------------------------
@@ -755,8 +860,16 @@ template <class W, bool PRED, int MODE>
 __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
   using L = Label<PRED>;
   __shared__ PhaseRec s_rec;
+  extern __shared__ uint32_t s_stage[];   // kStageWords per warp
   Tally t;
   t.keep = l2_keep_policy();
+  {
+    uint32_t* wb = s_stage + (threadIdx.x >> 5) * kStageWords;
+    t.q.nearb = wb;
+    t.q.farb = wb + kNearBuf;
+    t.q.slotb = wb + kNearBuf + kFarBuf;
+    t.q.memb = wb + kNearBuf + kFarBuf + 2 * kSlotBuf;
+  }
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   Control* c = P.ctl;
@@ -925,7 +1038,8 @@ int max_grid() {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sssp<W, PRED, MODE>, kThreads, 0);
+  cudaFuncSetAttribute(k_sssp<W, PRED, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sssp<W, PRED, MODE>, kThreads, kStageBytes);
   if (per < 1) per = 1;
   cached = per * sms;
   return cached;
@@ -935,7 +1049,8 @@ template <class W, bool PRED, int MODE>
 cudaError_t launch(const Params& P, int grid, cudaStream_t st) {
   Params copy = P;
   void* args[] = {&copy};
-  return cudaLaunchCooperativeKernel((void*)k_sssp<W, PRED, MODE>, dim3(grid), dim3(kThreads), args, 0, st);
+  return cudaLaunchCooperativeKernel((void*)k_sssp<W, PRED, MODE>, dim3(grid), dim3(kThreads), args, kStageBytes,
+                                     st);
 }
 
 b2_status map_device_error(uint32_t e) {
