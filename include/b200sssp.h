@@ -205,6 +205,16 @@ b2_status b2_minplus_gemm_i32(const int32_t* dA, const int32_t* dB, int32_t* dC,
  * nothing.  *squarings_out = products computed. */
 b2_status b2_apsp_f32(float* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
 b2_status b2_apsp_i32(int32_t* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
+/* b2_apsp_f32 without any device allocation, for callers that cannot call
+ * cudaMalloc while they run (a plugin whose host owns the device memory pool,
+ * a serving loop with a fixed memory budget).  No counterpart in the
+ * reference.  Its scratch is a fixed 16 MiB module array, so N <= 2048
+ * (larger N returns B2_NOT_SUPPORTED); each GPU that loads the library holds
+ * that array until exit.  All calls on a device share it: calls that overlap
+ * on the GPU race and must be serialized by the caller.  The first call on a
+ * device resolves the array's device address; make it before any stream
+ * capture. */
+b2_status b2_apsp_f32_noalloc(float* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
 /* Sustained (min,+) pairs per second of this GPU's CUDA cores, measured by a
  * register-only kernel of the same instruction mix as the GEMM inner loop
  * (int32: DPX add-min; fp32: FADD + three-input min).  The roofline

@@ -453,3 +453,93 @@ extern "C" b2_status b2_minplus_calibrate(int32_t is_float, double* pairs_per_se
   *pairs_per_second = (double)blocks * threads * iters * 16.0 / (best * 1e-3);
   return B2_SUCCESS;
 }
+
+// ---- allocation-free APSP --------------------------------------------------
+// Some callers cannot allocate device memory while they run:
+//   * a plugin inside a host whose device memory is owned by another
+//     allocator (a framework's caching pool), where a cudaMalloc would
+//     fragment or exceed that pool's budget;
+//   * a latency-bound serving loop with a fixed memory budget, where
+//     cudaMalloc / cudaFree would synchronize the device and add jitter;
+//   * code running while a device-wide allocation freeze is in effect.
+// b2_apsp_f32_noalloc runs the same repeated squaring as b2_apsp_f32, but its
+// ping-pong matrix and change flag live in the fixed array below instead of a
+// cudaMalloc'd buffer.  Limits and rules:
+//   * N * N * 4 bytes must fit in the array (N <= 2048); larger N is rejected
+//     with B2_NOT_SUPPORTED before anything runs;
+//   * the array is a module global: every GPU that loads this library holds
+//     its 16 MiB until the process exits;
+//   * every call on a device shares the one array, and it keeps the previous
+//     call's contents (the change flag is cleared before each product): calls
+//     that overlap on the GPU (different streams or threads) race and must be
+//     serialized by the caller;
+//   * the first call on each device looks up the array's device address
+//     (cudaGetSymbolAddress) with that device current; make that first call
+//     before any stream capture.
+namespace b2 {
+namespace {
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;   // 16 MiB: 2048 x 2048 floats
+// scratch matrix, then the change flag in the last 256 bytes
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes + 256];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+// Device address of g_noalloc_scratch for the current device (looked up once
+// per device; the host-side symbol itself is not a device address).
+cudaError_t noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = (unsigned char*)g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+}  // namespace
+}  // namespace b2
+
+extern "C" b2_status b2_apsp_f32_noalloc(float* d_D, int32_t N, b2_stream stream, int32_t* squarings) {
+  using namespace b2;
+  if (!d_D || N <= 0) return B2_INVALID_ARGUMENT;
+  if ((size_t)N * (size_t)N * sizeof(float) > kNoAllocScratchBytes) return B2_NOT_SUPPORTED;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (squarings) *squarings = 0;
+  if (N == 1) return B2_SUCCESS;
+  unsigned char* base = nullptr;
+  B2_CUDA_TRY(noalloc_scratch(&base));
+  float* tmp = (float*)base;
+  uint32_t* flag = (uint32_t*)(base + kNoAllocScratchBytes);
+  int maxsq = 0;
+  while ((1ll << maxsq) < (long long)(N - 1)) ++maxsq;
+  float* cur = d_D;
+  float* nxt = tmp;
+  int done = 0;
+  cudaError_t e = cudaSuccess;
+  for (int it = 0; it < maxsq; ++it) {
+    uint32_t hflag = 0;
+    e = cudaMemsetAsync(flag, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = launch_minplus<float>(cur, cur, nxt, N, N, N, N, N, N, st, cur, flag);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) break;
+    ++done;
+    std::swap(cur, nxt);
+    if (hflag == 0) break;
+  }
+  if (e == cudaSuccess && cur != d_D) {
+    e = cudaMemcpyAsync(d_D, cur, (size_t)N * N * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  if (squarings) *squarings = done;
+  if (e != cudaSuccess) return from_cuda(e);
+  uint32_t err = 0;
+  cudaMemcpyFromSymbol(&err, g_mp_error, sizeof(err));
+  return err ? B2_TIMEOUT : B2_SUCCESS;
+}
