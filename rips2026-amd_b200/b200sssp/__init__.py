@@ -248,6 +248,21 @@ class Graph:
             pass
 
 
+def bf_dense(adj, source: int, out=None, stream=None, **opts):
+    """Bellman-Ford over a dense incoming adjacency (adj[v, u] = w(u->v), +inf = no edge)
+    on the GPU; returns (dist tensor, stats dict)."""
+    torch = _torch()
+    if adj.dim() != 2 or adj.shape[0] != adj.shape[1] or adj.dtype != torch.float32 or not adj.is_contiguous():
+        raise ValueError("square contiguous float32 CUDA matrix required")
+    n = adj.shape[0]
+    dist = out if out is not None else torch.empty(n, dtype=torch.float32, device=adj.device)
+    o = default_opts(**opts)
+    st = _lib.Stats()
+    check(lib().b2_sssp_bf_dense(C.c_void_p(adj.data_ptr()), n, source, C.c_void_p(dist.data_ptr()), C.byref(o),
+                                 C.c_void_p(_stream_ptr(stream)), C.byref(st)), "bf_dense")
+    return dist, st.as_dict()
+
+
 def dist_to_numpy(dist, weight: str) -> np.ndarray:
     """Device distances -> float64 numpy with +inf for unreachable."""
     a = dist.cpu().numpy()

@@ -1,0 +1,85 @@
+"""GPU parity: CSR x CSR min-plus SpGEMM vs the oracle (bit-exact; sorted rows)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+MISS = 1073741823
+
+
+def _rand_csr(rng, R, C, dens, dtype, dup=False):
+    rows, cols, vals = [], [], []
+    for r in range(R):
+        k = rng.binomial(C, dens) if C else 0
+        cs = rng.choice(C, size=k, replace=False) if k else np.zeros(0, int)
+        if dup and k:
+            cs = np.concatenate([cs, rng.choice(cs, size=max(1, k // 3))])
+        rng.shuffle(cs)
+        rows += [r] * len(cs)
+        cols += cs.tolist()
+        if dtype == np.float32:
+            v = rng.uniform(0, 1, len(cs)).astype(np.float32)
+            v[rng.uniform(size=len(cs)) < 0.05] = np.inf
+            v[rng.uniform(size=len(cs)) < 0.03] = np.nan
+        else:
+            v = rng.integers(1, 1001, len(cs)).astype(np.int32)
+            v[rng.uniform(size=len(cs)) < 0.1] = MISS
+        vals += v.tolist()
+    rp = np.zeros(R + 1, np.int64)
+    np.add.at(rp, np.array(rows, np.int64) + 1, 1)
+    return np.cumsum(rp), np.array(cols, np.int32), np.array(vals, dtype)
+
+
+def _gpu(b2, torch, A, B, ncols_b):
+    ta = (torch.from_numpy(A[0]).cuda(), torch.from_numpy(A[1]).cuda(), torch.from_numpy(A[2]).cuda(),
+          int(B[0].shape[0] - 1))
+    tb = (torch.from_numpy(B[0]).cuda(), torch.from_numpy(B[1]).cuda(), torch.from_numpy(B[2]).cuda(), ncols_b)
+    rp, ci, v = b2.minplus_spgemm(ta, tb)
+    return rp.cpu().numpy(), ci.cpu().numpy(), v.cpu().numpy()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.int32])
+@pytest.mark.parametrize("shape", [(40, 30, 50, 0.2), (200, 150, 120, 0.05), (1, 1, 1, 1.0), (64, 64, 64, 0.0),
+                                   (300, 40, 500, 0.3)])
+def test_spgemm_matches_oracle(b2, orc, cuda, dtype, shape):
+    M, K, N, d = shape
+    rng = np.random.default_rng(M + K + N)
+    A = _rand_csr(rng, M, K, d, dtype, dup=True)
+    B = _rand_csr(rng, K, N, d, dtype, dup=True)
+    got = _gpu(b2, cuda, A, B, N)
+    ref = orc.minplus_spgemm(A, B, N)
+    assert np.array_equal(got[0], ref[0])
+    assert np.array_equal(got[1], ref[1])
+    assert np.array_equal(got[2], ref[2])
+
+
+def test_spgemm_graph_square(b2, orc, cuda):
+    """A (x) A on an ER graph: two-hop shortest path lengths (config C2s shape, scaled down)."""
+    g = b2.gen_er(1 << 14, 8 << 14, 1, 1000, 5)
+    A = (g.rowptr, g.colind, g.weights.astype(np.int32))
+    got = _gpu(b2, cuda, A, A, g.n)
+    ref = orc.minplus_spgemm(A, A, g.n)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+    Af = (g.rowptr, g.colind, g.fweights)
+    got = _gpu(b2, cuda, Af, Af, g.n)
+    ref = orc.minplus_spgemm(Af, Af, g.n)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+
+
+def test_spgemm_invalid_inputs(b2, cuda):
+    torch = cuda
+    rp = torch.tensor([0, 1, 2], dtype=torch.int64, device="cuda")
+    ci = torch.tensor([0, 5], dtype=torch.int32, device="cuda")         # 5 >= K
+    v = torch.tensor([1.0, 2.0], dtype=torch.float32, device="cuda")
+    good_ci = torch.tensor([0, 1], dtype=torch.int32, device="cuda")
+    with pytest.raises(b2.B2Error) as e:
+        b2.minplus_spgemm((rp, ci, v, 2), (rp, good_ci, v, 2))
+    assert e.value.status == 9
+    bad_rp = torch.tensor([0, 2, 1], dtype=torch.int64, device="cuda")
+    with pytest.raises(b2.B2Error) as e:
+        b2.minplus_spgemm((bad_rp, good_ci, v, 2), (rp, good_ci, v, 2))
+    assert e.value.status == 10
+    with pytest.raises(b2.B2Error) as e:      # A.cols != B.rows
+        b2.minplus_spgemm((rp, good_ci, v, 3), (rp, good_ci, v, 2))
+    assert e.value.status == 1

@@ -263,3 +263,27 @@ def test_phase_trace(b2, cuda):
     assert any(e["kind"] == "relax-heavy" for e in tr)
     _, _, st = g.sssp(0, method="bf", trace=1)
     assert len(g.trace()) == st["phases"]
+
+
+def test_dense_bf_known_answers(b2, golden, cuda):
+    """bellman_ford_minplus_hip's dense path on the reference's 14 KATs
+    (HIP_kernel/bellman_ford/tests/test_correctness.cpp), n <= 1024 dense."""
+    torch = cuda
+    z = golden("dense_kats.npz")
+    for name in [str(x) for x in z["names"]]:
+        n, src, py_iters = (int(x) for x in z[f"{name}/meta"])
+        if n > 1024:
+            continue
+        adj = np.full((n, n), np.inf, np.float32)
+        for u, v, w in z[f"{name}/edges"]:
+            u, v = int(u), int(v)
+            adj[v, u] = min(adj[v, u], np.float32(w))
+        dist, st = b2.bf_dense(torch.from_numpy(adj).cuda(), src)
+        got = _np(dist).astype(np.float64)
+        exp = z[f"{name}/expected"]
+        both = np.isinf(got) & np.isinf(exp)
+        with np.errstate(invalid="ignore"):
+            ok = both | (np.abs(got - exp) <= 1e-4 * (1 + np.abs(got) + np.abs(exp)))
+        assert ok.all(), name
+        if n > 1:
+            assert st["iterations_used"] == py_iters, name
