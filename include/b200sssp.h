@@ -131,7 +131,8 @@ typedef struct b2_sssp_opts {
 } b2_sssp_opts;
 
 typedef struct b2_trace_entry {
-  uint32_t kind;        /* 1 relax, 2 commit, 3 far split, 4 probe, 5 output; | 0x100 heavy pass */
+  uint32_t kind;        /* 1 relax, 2 commit, 3 far split, 4 probe, 5 output, 7 fused (one block);
+                           | 0x100 heavy pass */
   uint32_t frontier;    /* frontier entries of the phase */
   uint32_t hub_chunks;  /* 256-edge chunks of split high-degree vertices */
   uint32_t bucket;      /* delta: bucket index; BF: round */
@@ -153,7 +154,8 @@ typedef struct b2_stats {
   uint32_t device_error;
   uint32_t grid_blocks;
   uint32_t first_unchanged; /* BF: first round that changed nothing (0: none observed) */
-  uint32_t reserved[5];
+  uint32_t local_subphases; /* delta/ADDS: sub-phases run by one block under bucket fusion */
+  uint32_t reserved[4];
 } b2_stats;
 
 /* ---- library ---------------------------------------------------------- */

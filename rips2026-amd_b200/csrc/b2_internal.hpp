@@ -80,6 +80,7 @@ enum PhaseKind : uint32_t {
   kPhaseProbe = 4,     // delta: count valid pending entries (max_iters cut)
   kPhaseFinal = 5,     // write outputs
   kPhaseDone = 6,
+  kPhaseLocal = 7,     // delta: block 0 alone runs small light sub-phases (bucket fusion)
 };
 
 enum QueueId : uint32_t {
@@ -111,6 +112,10 @@ struct Control {
   uint32_t probe_valid;    // PROBE phase result
   uint32_t members_count;  // entries in the heavy-round member list
   uint32_t trace_n;
+  uint32_t stamp_ctr;      // next dedup stamp (manager and local loop)
+  uint32_t local_q;        // LOCAL phase: queue holding the next frontier
+  uint32_t local_iters;    // LOCAL phase: sub-phases run inside it
+  uint32_t local_total;    // sub-phases run by all LOCAL phases
   // results
   uint32_t iterations;
   uint32_t converged;

@@ -83,6 +83,7 @@ struct Params {
   int32_t* out_pred;
   uint32_t dist_is_out;   // `dist` aliases out_dist (no separate label buffer)
   uint32_t is_float;
+  uint32_t fusion;        // light frontiers up to this size run as a LOCAL phase (0: off)
 };
 
 // ---------------------------------------------------------------------------
@@ -484,7 +485,8 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
   uint32_t deg = valid ? (uint32_t)min(hi - lo, (uint64_t)0xFFFFFFFFull) : 0u;
   // high-degree ranges -> one hub-list entry per 256-edge chunk, written by
   // the whole warp, taken by any warp in the next phase
-  uint32_t hubs = __ballot_sync(0xffffffffu, deg >= P.hub_degree);
+  const uint32_t hub_deg = R.kind == kPhaseLocal ? 0xFFFFFFFFu : P.hub_degree;
+  uint32_t hubs = __ballot_sync(0xffffffffu, deg >= hub_deg);
   while (hubs) {
     const uint32_t hl = __ffs(hubs) - 1;
     hubs &= hubs - 1;
@@ -626,6 +628,7 @@ __device__ void manager_init(const Params& P) {
   r.fcount = 1;
   r.push_q = kQNear1;
   r.stamp = P.phase_base + 1;
+  c->stamp_ctr = 2;
   r.hround = P.phase_base + 1;
   r.hub_in = 1;
   r.hub_out = 0;
@@ -645,6 +648,12 @@ __device__ __forceinline__ bool over_budget(const Params& P, PhaseRec& nx) {
     return true;
   }
   return false;
+}
+
+__device__ __forceinline__ void consume_queue(Control* c, uint32_t fq) {
+  if (fq == kQNear0 || fq == kQNear1) c->near_count[fq] = 0;
+  else if (fq == kQMembers) c->members_count = 0;
+  else if (fq >= kQSlot0 && fq < kQSlot0 + kRing) c->slot_count[fq - kQSlot0] = 0;
 }
 
 __device__ __forceinline__ void consume_process_counters(Control* c, const PhaseRec& r) {
@@ -673,7 +682,7 @@ __device__ void manager_bf(const Params& P) {
     nx.fq = r.fq;
     nx.fcount = r.fcount;
     nx.push_q = r.fq ^ 1u;
-    nx.stamp = P.phase_base + nx.phase;
+    nx.stamp = P.phase_base + (c->stamp_ctr++);
     nx.hub_in = r.hub_out ^ 1u;
     nx.hub_in_count = 0;
     nx.hub_in_chunks = 0;
@@ -734,7 +743,7 @@ __device__ void manager_delta(const Params& P) {
   trace_phase(P, r, r.cur);
   PhaseRec nx = r;
   nx.phase = r.phase + 1;
-  nx.stamp = P.phase_base + nx.phase;
+  nx.stamp = P.phase_base + (c->stamp_ctr++);
   c->phases = vld(&c->phases) + 1;
   if (r.kind == kPhaseFinal) { nx.kind = kPhaseDone; store_rec(c, nx); return; }
   if (over_budget(P, nx)) return;
@@ -753,7 +762,17 @@ __device__ void manager_delta(const Params& P) {
     c->far_min = vld(&c->far_min_next);
     c->far_min_next = 0xFFFFFFFFu;
     from_slot = 0;
-  } else {  // PROCESS (light or heavy)
+  } else {  // PROCESS (light or heavy) or LOCAL
+    PhaseRec rr = r;
+    if (r.kind == kPhaseLocal) {
+      // the local loop consumed every frontier it ran; its last pushes sit in local_q
+      rr.fq = kQNone;
+      rr.hub_in_chunks = 0;
+      rr.push_q = vld(&c->local_q);
+      rr.heavy = 0;
+      c->local_total = vld(&c->local_total) + vld(&c->local_iters);
+    }
+    const PhaseRec& r = rr;
     consume_process_counters(c, r);
     const uint32_t hch = vld(&c->hub_count[r.hub_out & 1]);
     const uint32_t hcnt = hch;
@@ -771,6 +790,7 @@ __device__ void manager_delta(const Params& P) {
         return;
       }
       if (nn > 0) {              // a heavy relaxation landed in this bucket: new light round
+        nx.kind = kPhaseProcess;
         nx.heavy = 0;
         nx.fq = r.push_q;
         nx.fcount = nn;
@@ -781,14 +801,17 @@ __device__ void manager_delta(const Params& P) {
       }
     } else {
       if (nn > 0 || hch > 0) {
+        nx.kind = kPhaseProcess;
         nx.fq = nn ? r.push_q : kQNone;
         nx.fcount = nn;
         nx.push_q = r.push_q ^ 1u;
+        if (hch == 0 && nn <= P.fusion) nx.kind = kPhaseLocal;
         store_rec(c, nx);
         return;
       }
       const uint32_t mc = vld(&c->members_count);
       if (mc > 0) {              // light rounds of this bucket are done: heavy pass
+        nx.kind = kPhaseProcess;
         nx.heavy = 1;
         nx.fq = kQMembers;
         nx.fcount = mc;
@@ -832,6 +855,7 @@ __device__ void manager_delta(const Params& P) {
     nx.fq = kQSlot0 + (uint32_t)found;
     nx.fcount = cnts[found];
     nx.push_q = kQNear0;   // both near queues are empty at a bucket boundary
+    if (nx.fcount <= P.fusion) nx.kind = kPhaseLocal;
     store_rec(c, nx);
     return;
   }
@@ -853,6 +877,52 @@ __device__ void manager_delta(const Params& P) {
   c->converged = 1;
   nx.kind = kPhaseFinal;
   store_rec(c, nx);
+}
+
+// Bucket fusion: block 0 alone runs consecutive light sub-phases of one
+// bucket while the frontier stays at or under P.fusion, separated by block
+// barriers instead of grid barriers; every other block waits at the next grid
+// barrier.  Same relaxation code, same dedup stamps (drawn from the shared
+// stamp counter), no hub splitting.  Exits when the frontier empties or grows
+// past the threshold; the manager continues from local_q.
+constexpr uint32_t kMaxLocalIters = 1u << 16;
+
+template <class W, bool PRED, int MODE>
+__device__ void local_phase(const Params& P, const PhaseRec& R0, Tally& t) {
+  __shared__ uint32_t s_l[5];
+  Control* c = P.ctl;
+  PhaseRec L = R0;
+  const uint32_t w = threadIdx.x >> 5;
+  const uint32_t nw = blockDim.x >> 5;
+  for (uint32_t iter = 0;; ++iter) {
+    const uint32_t nfc = (L.fcount + 31) / 32;
+    for (uint32_t ch = w; ch < nfc; ch += nw) frontier_chunk<W, PRED, MODE>(P, L, ch * 32, t);
+    flush_all<MODE>(P, L, t.q, true);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      consume_queue(c, L.fq);
+      const uint32_t nn = ldcg(&c->near_count[L.push_q & 1]);
+      const bool budget = globaltimer_ns() - c->t_start > P.budget_ns;
+      if (budget) atomicCAS(&c->error, kErrNone, (uint32_t)kErrTimeout);
+      uint32_t done = (nn == 0 || nn > P.fusion || iter + 1 >= kMaxLocalIters || budget) ? 1u : 0u;
+      if (!done) {
+        s_l[0] = L.push_q;
+        s_l[1] = nn;
+        s_l[2] = L.push_q ^ 1u;
+        s_l[3] = P.phase_base + (c->stamp_ctr++);
+      }
+      s_l[4] = done;
+      c->local_q = L.push_q;
+      c->local_iters = iter + 1;
+    }
+    __syncthreads();
+    if (s_l[4]) break;
+    L.fq = s_l[0];
+    L.fcount = s_l[1];
+    L.push_q = s_l[2];
+    L.stamp = s_l[3];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -892,6 +962,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
     R.fcount = min(R.fcount, P.n);
     if (R.kind == kPhaseProcess) {
       process_phase<W, PRED, MODE>(P, R, t);
+    } else if (R.kind == kPhaseLocal) {
+      if (MODE == kModeDelta && blockIdx.x == 0) local_phase<W, PRED, MODE>(P, R, t);
     } else if (R.kind == kPhaseCommit) {
       const uint32_t* F = queue_ptr(P, R.fq);
       for (size_t i = tid; i < R.fcount; i += stride) {
@@ -1143,6 +1215,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
       delta = (double)P.delta_u;
     }
     P.max_iters = o.max_iters < 0 ? 0xFFFFFFFFu : (uint32_t)o.max_iters;
+    P.fusion = o.fusion_threshold;
     if (o.light_heavy && g->rows_sorted) {
       s = ensure_light_counts(g, isf, P.delta_u, df, st);
       if (s != B2_SUCCESS) return s;
@@ -1209,7 +1282,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return from_cuda(e);
   const Control& hc = *w.h_ctl;
-  w.phase_epoch += hc.rec.phase + 2;
+  w.phase_epoch += std::max(hc.rec.phase, hc.stamp_ctr) + 2;
   w.trace_n = o.trace ? hc.trace_n : 0;
   b2_status ds = map_device_error(hc.error);
   if (stats) {
@@ -1224,6 +1297,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     stats->device_error = hc.error;
     stats->grid_blocks = (uint32_t)grid;
     stats->first_unchanged = hc.first_unchanged;
+    stats->local_subphases = hc.local_total;
   }
   if (ds != B2_SUCCESS) return ds;
   if (stats && o.collect_reach) {

@@ -287,3 +287,26 @@ def test_dense_bf_known_answers(b2, golden, cuda):
         assert ok.all(), name
         if n > 1:
             assert st["iterations_used"] == py_iters, name
+
+
+@pytest.mark.parametrize("fusion", [64, 4096, 1 << 30])
+def test_bucket_fusion_is_schedule_only(b2, orc, cuda, fusion):
+    """Small light frontiers run by one block (bucket fusion) give the same
+    distances, predecessor trees and bucket counts as the grid-wide schedule."""
+    for hg, weight, delta in ((b2.gen_grid(80, 70, 0.02, seed=31), "u32", 500.0),
+                              (b2.gen_rmat(12, 16, seed=32), "f32", 0.1),
+                              (b2.gen_er(3000, 15000, 1, 50, 33), "u32", 7.0)):
+        g = _graph(b2, hg, weight)
+        w = hg.weights if weight == "u32" else hg.fweights
+        d0, _, s0 = g.sssp(1, method="delta", delta=delta, fusion_threshold=0)
+        d1, p1, s1 = g.sssp(1, method="delta", delta=delta, fusion_threshold=fusion, pred=True)
+        assert np.array_equal(_np(d0), _np(d1))
+        assert s0["iterations_used"] == s1["iterations_used"]
+        assert s1["local_subphases"] > 0
+        got = _dist_u32(d1) if weight == "u32" else _np(d1)
+        assert np.array_equal(got, orc.dijkstra(hg.rowptr, hg.colind, w, 1))
+        assert orc.validate_spt(hg.rowptr, hg.colind, w, 1, got, _np(p1)) == 0
+        dk, _, sk = g.sssp(1, method="delta", delta=delta, fusion_threshold=fusion, max_iters=3)
+        dr, _, sr = g.sssp(1, method="delta", delta=delta, fusion_threshold=0, max_iters=3)
+        assert np.array_equal(_np(dk), _np(dr)) and sk["converged"] == sr["converged"]
+        g.close()
