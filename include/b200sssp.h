@@ -155,7 +155,9 @@ typedef struct b2_stats {
   uint32_t grid_blocks;
   uint32_t first_unchanged; /* BF: first round that changed nothing (0: none observed) */
   uint32_t local_subphases; /* delta/ADDS: sub-phases run by one block under bucket fusion */
-  uint32_t reserved[4];
+  uint32_t delta_updates;   /* ADDS: bucket-width changes */
+  double delta_final;       /* ADDS: bucket width at the end (delta: = delta_used) */
+  uint32_t reserved[2];
 } b2_stats;
 
 /* ---- library ---------------------------------------------------------- */

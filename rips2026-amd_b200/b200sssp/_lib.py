@@ -67,7 +67,8 @@ class Stats(C.Structure):
                 ("pushes", C.c_uint64), ("reached", C.c_uint64), ("reached_edges", C.c_uint64),
                 ("delta_used", C.c_double), ("kernel_ms", C.c_float), ("device_error", C.c_uint32),
                 ("grid_blocks", C.c_uint32), ("first_unchanged", C.c_uint32),
-                ("local_subphases", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("local_subphases", C.c_uint32), ("delta_updates", C.c_uint32),
+                ("delta_final", C.c_double), ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -59,7 +59,10 @@ struct PhaseRec {
   uint32_t heavy;       // 1: relax the heavy suffix (w > delta) of each frontier vertex
   uint32_t hround;      // stamp of the current heavy round (members dedup)
   uint32_t aux;         // BF: round role (0 normal, 2 commit-before-probe, 1 probe); FINAL: source buffer
-  uint32_t pad;
+  uint32_t dq;          // bucket width (uint32 graphs)
+  uint32_t dinv;        // float bits of 1/width (float graphs)
+  uint32_t dbase;       // distance key at which bucket dbase_b starts (0 until re-based)
+  uint32_t dbase_b;
 };
 
 // One entry per executed phase when tracing is on (manager-written).
@@ -116,6 +119,11 @@ struct Control {
   uint32_t local_q;        // LOCAL phase: queue holding the next frontier
   uint32_t local_iters;    // LOCAL phase: sub-phases run inside it
   uint32_t local_total;    // sub-phases run by all LOCAL phases
+  uint32_t far_min_key;    // adaptive mode: min distance key that landed in the far pile
+  uint32_t far_min_key_next;
+  unsigned long long win_frontier_sum;   // adaptive mode: frontier entries in this window
+  uint32_t win_phases;
+  uint32_t delta_updates;
   // results
   uint32_t iterations;
   uint32_t converged;

@@ -84,6 +84,8 @@ struct Params {
   uint32_t dist_is_out;   // `dist` aliases out_dist (no separate label buffer)
   uint32_t is_float;
   uint32_t fusion;        // light frontiers up to this size run as a LOCAL phase (0: off)
+  uint32_t adapt;         // ADDS: adjust the bucket width at window boundaries
+  uint32_t adapt_cap;     // ADDS: frontier entries the grid takes per phase (utilization base)
 };
 
 // ---------------------------------------------------------------------------
@@ -107,15 +109,25 @@ struct Label<true> {
   static constexpr T kInf = 0xFFFFFFFFFFFFFFFFull;
 };
 
+// Bucket of a distance key under the phase's mapping
+//   bucket = dbase_b + floor((d - dbase) / width).
+// With dbase = 0 and dbase_b = 0 (delta-stepping; ADDS before its first
+// re-basing) this is the reference rule: d / delta for uint32 and
+// floorf(d * (1.0f / delta)) clamped to [0, kNoBucket) for float.  Keys below
+// dbase belong to settled buckets and map to dbase_b - 1.
 template <class W>
-__device__ __forceinline__ uint32_t bucket_of(const Params& P, uint32_t key) {
-  if (!W::kFloat) return key / P.delta_u;
+__device__ __forceinline__ uint32_t bucket_of(const PhaseRec& R, uint32_t key) {
+  if (!W::kFloat) {
+    if (key < R.dbase) return R.dbase_b ? R.dbase_b - 1 : 0;
+    const uint32_t b = (key - R.dbase) / R.dq;
+    return R.dbase_b + b;
+  }
   const float d = key_to_f32(key);
   if (!isfinite(d)) return kNoBucket;
-  const float bf = floorf(d * P.inv_delta);
-  if (bf < 0.0f) return 0;
-  if (bf >= (float)kNoBucket) return kNoBucket - 1;
-  return (uint32_t)bf;
+  const float bf = floorf((d - __uint_as_float(R.dbase)) * __uint_as_float(R.dinv));
+  if (bf < 0.0f) return (R.dbase_b && R.dbase) ? R.dbase_b - 1 : R.dbase_b;
+  if (bf + (float)R.dbase_b >= (float)kNoBucket) return kNoBucket - 1;
+  return R.dbase_b + (uint32_t)bf;
 }
 
 __device__ __forceinline__ uint32_t* queue_ptr(const Params& P, uint32_t id) {
@@ -324,7 +336,7 @@ __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool i
   uint32_t b = 0;
   int cls = 0;  // 1 near, 2 window slot, 3 far
   if (improved) {
-    b = bucket_of<W>(P, cand);
+    b = bucket_of<W>(R, cand);
     if (b <= R.cur) cls = 1;
     else if (b < R.win + (uint32_t)kRing) cls = 2;
     else cls = 3;
@@ -354,6 +366,10 @@ __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool i
     }
     bmin = __reduce_min_sync(0xffffffffu, bmin);
     if (lane_id() == 0 && bmin != 0xFFFFFFFFu) atomicMin(&c->far_min, bmin);
+    if (P.adapt) {
+      const uint32_t kmin = __reduce_min_sync(0xffffffffu, cls == 3 ? cand : 0xFFFFFFFFu);
+      if (lane_id() == 0 && kmin != 0xFFFFFFFFu) atomicMin(&c->far_min_key, kmin);
+    }
     stage(t.q.farb, t.q.nf, want, v);
     t.pushes += want ? 1 : 0;
   }
@@ -428,7 +444,7 @@ __device__ __forceinline__ void hub_chunk(const Params& P, const PhaseRec& R, ui
   const uint32_t v = h.x;
   const uint32_t du = src_key<W, PRED, MODE>(P, v);
   bool valid = du != kInfKey;
-  if (MODE == kModeDelta) valid = valid && bucket_of<W>(P, du) == R.cur;
+  if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
   if (!valid) return;
   uint64_t rlo, rhi;
   bool hh;
@@ -467,7 +483,7 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
     v = ldcg(F + i);
     du = src_key<W, PRED, MODE>(P, v);
     valid = du != kInfKey;
-    if (MODE == kModeDelta) valid = valid && bucket_of<W>(P, du) == R.cur;
+    if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
     if (valid) phase_range(P, R, v, lo, hi, has_heavy);
   }
   if (MODE == kModeDelta) {
@@ -633,6 +649,12 @@ __device__ void manager_init(const Params& P) {
   r.hub_in = 1;
   r.hub_out = 0;
   r.iter = 1;
+  r.dq = P.delta_u;
+  r.dinv = __float_as_uint(P.inv_delta);
+  r.dbase = 0;
+  r.dbase_b = 0;
+  c->far_min_key = 0xFFFFFFFFu;
+  c->far_min_key_next = 0xFFFFFFFFu;
   store_rec(c, r);
 }
 
@@ -756,11 +778,17 @@ __device__ void manager_delta(const Params& P) {
   uint32_t win = r.win;
   uint32_t far_sel = r.far_sel;
   uint32_t from_slot = 0;   // first window slot to look at
+  if ((r.kind == kPhaseProcess || r.kind == kPhaseLocal) && !r.heavy) {
+    c->win_frontier_sum = c->win_frontier_sum + r.fcount;
+    c->win_phases = vld(&c->win_phases) + 1;
+  }
   if (r.kind == kPhaseSplit) {
     c->far_count[r.far_sel] = 0;
     far_sel = r.far_sel ^ 1u;
     c->far_min = vld(&c->far_min_next);
     c->far_min_next = 0xFFFFFFFFu;
+    c->far_min_key = vld(&c->far_min_key_next);
+    c->far_min_key_next = 0xFFFFFFFFu;
     from_slot = 0;
   } else {  // PROCESS (light or heavy) or LOCAL
     PhaseRec rr = r;
@@ -861,16 +889,41 @@ __device__ void manager_delta(const Params& P) {
   }
   const uint32_t fc = vld(&c->far_count[far_sel]);
   if (fc > 0) {
-    const uint32_t fmin = vld(&c->far_min);
+    const uint32_t fmin_b = vld(&c->far_min);
     uint32_t nwin = win + kRing;
-    const uint32_t aligned = (fmin / kRing) * kRing;
-    if (fmin != 0xFFFFFFFFu && aligned > nwin) nwin = aligned;
+    if (P.adapt) {
+      // ADDS feedback (hip_adds_sssp.hpp:41-56): widen buckets when the last
+      // window's frontiers left the grid under-used, narrow them when they
+      // overflowed it; the new window starts at the smallest far distance.
+      const unsigned long long ph = vld(&c->win_phases);
+      const double avg = ph ? (double)c->win_frontier_sum / (double)ph : 0.0;
+      double f = 1.0;
+      if (avg < 0.35 * (double)P.adapt_cap) f = 1.5;
+      else if (avg > 0.85 * (double)P.adapt_cap) f = 0.75;
+      if (f != 1.0) c->delta_updates = vld(&c->delta_updates) + 1;
+      if (P.is_float) {
+        const float wnew = fmaxf(1.0e-6f, (float)((1.0 / (double)__uint_as_float(r.dinv)) * f));
+        nx.dinv = __float_as_uint(1.0f / wnew);
+      } else {
+        const double wnew = fmax(1.0, floor((double)r.dq * f + 0.5));
+        nx.dq = (uint32_t)fmin(wnew, 4294967295.0);
+      }
+      const uint32_t kmin = vld(&c->far_min_key);
+      nx.dbase = kmin == 0xFFFFFFFFu ? r.dbase : (P.is_float ? __float_as_uint(key_to_f32(kmin)) : kmin);
+      nx.dbase_b = nwin;
+      c->win_frontier_sum = 0;
+      c->win_phases = 0;
+    } else {
+      const uint32_t aligned = (fmin_b / kRing) * kRing;
+      if (fmin_b != 0xFFFFFFFFu && aligned > nwin) nwin = aligned;
+    }
     nx.kind = kPhaseSplit;
     nx.fq = kQFar0 + far_sel;
     nx.fcount = fc;
     nx.win = nwin;
     nx.cur = nwin;
     c->far_min_next = 0xFFFFFFFFu;
+    c->far_min_key_next = 0xFFFFFFFFu;
     store_rec(c, nx);
     return;
   }
@@ -977,13 +1030,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
         const size_t i = base + lane_id();
         int cls = 0;
         uint32_t v = 0, b = 0;
+        uint32_t k = 0xFFFFFFFFu;
         if (i < R.fcount) {
           v = ldcg(F + i);
-          const uint32_t k = L::key(ldcg((const typename L::T*)P.dist + v));
-          b = bucket_of<W>(P, k);
+          k = L::key(ldcg((const typename L::T*)P.dist + v));
+          b = bucket_of<W>(R, k);
           if (b < R.win) { cls = 0; P.farflag[v] = 0u; }
-          else if (b < R.win + (uint32_t)kRing) { cls = 2; P.farflag[v] = 0u; }
-          else { cls = 3; kmin = min(kmin, b); }
+          else if (b < R.win + (uint32_t)kRing) { cls = 2; P.farflag[v] = 0u; P.bstamp[v] = b; }
+          else { cls = 3; kmin = min(kmin, b); P.bstamp[v] = b; }
+        }
+        if (P.adapt) {
+          const uint32_t km = __reduce_min_sync(0xffffffffu, cls == 3 ? k : 0xFFFFFFFFu);
+          if (lane_id() == 0 && km != 0xFFFFFFFFu) atomicMin(&c->far_min_key_next, km);
         }
         if (cls == 2) {
           const uint32_t s = b - R.win;
@@ -1013,7 +1071,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
         for (size_t i = tid; i < cnt; i += stride) {
           const uint32_t v = ldcg(F + i);
           const uint32_t k = L::key(ldcg((const typename L::T*)P.dist + v));
-          if (k != kInfKey && bucket_of<W>(P, k) == R.win + s) { any = true; break; }
+          if (k != kInfKey && bucket_of<W>(R, k) == R.win + s) { any = true; break; }
         }
       }
       {
@@ -1022,7 +1080,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
         for (size_t i = tid; i < cnt && !any; i += stride) {
           const uint32_t v = ldcg(F + i);
           const uint32_t k = L::key(ldcg((const typename L::T*)P.dist + v));
-          if (k != kInfKey && bucket_of<W>(P, k) >= R.win + (uint32_t)kRing) any = true;
+          if (k != kInfKey && bucket_of<W>(R, k) >= R.win + (uint32_t)kRing) any = true;
         }
       }
       if (any) c->probe_valid = 1u;
@@ -1149,7 +1207,7 @@ b2_status ensure_light_counts(b2_graph g, bool isf, uint32_t delta_u, float delt
 }
 
 b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t* d_pred,
-                   const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats) {
+                   const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats, bool adds = false) {
   if (!g || !d_dist) return B2_INVALID_ARGUMENT;
   if ((int64_t)source >= g->n) return B2_INVALID_ARGUMENT;
   b2_sssp_opts o;
@@ -1216,6 +1274,14 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     }
     P.max_iters = o.max_iters < 0 ? 0xFFFFFFFFu : (uint32_t)o.max_iters;
     P.fusion = o.fusion_threshold;
+    if (adds) {
+      int dev = 0, sms = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      P.adapt = 1;
+      P.adapt_cap = (uint32_t)sms * 2u * (uint32_t)kThreads;
+      if (P.fusion == 0 && g->max_degree <= 64) P.fusion = 1024;   // low-degree graphs: fuse tails
+    }
     if (o.light_heavy && g->rows_sorted) {
       s = ensure_light_counts(g, isf, P.delta_u, df, st);
       if (s != B2_SUCCESS) return s;
@@ -1298,6 +1364,13 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     stats->grid_blocks = (uint32_t)grid;
     stats->first_unchanged = hc.first_unchanged;
     stats->local_subphases = hc.local_total;
+    stats->delta_updates = hc.delta_updates;
+    if (mode == kModeDelta) {
+      float inv;
+      memcpy(&inv, &hc.rec.dinv, 4);
+      stats->delta_final = isf ? 1.0 / (double)inv : (double)hc.rec.dq;
+    } else
+      stats->delta_final = delta;
   }
   if (ds != B2_SUCCESS) return ds;
   if (stats && o.collect_reach) {
@@ -1330,6 +1403,19 @@ extern "C" b2_status b2_sssp_bf(b2_graph g, uint32_t source, void* d_dist, int32
 extern "C" b2_status b2_sssp_delta(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
                                    const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats) {
   return run_sssp(g, kModeDelta, source, d_dist, d_pred, opts, (cudaStream_t)stream, stats);
+}
+
+// ADDS-style schedule (adds_sssp_hip, Charlotte_oneshot/sssp_hip.cpp:428-595;
+// hip_adds::sssp, jasper_oneshot_untested/hip_adds_sssp.cpp:1138-1301): the
+// delta-stepping machinery with the bucket width adapted at every window
+// boundary from measured frontier utilization (growth 1.5 / shrink 0.75 below
+// 35 % / above 85 % of the grid's per-phase capacity, the reference's
+// Options defaults) and small light frontiers fused into one block.  The
+// initial width is the Near-Far heuristic unless opts->delta is set.
+// iterations_used counts processed buckets of the adapted widths.
+extern "C" b2_status b2_sssp_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred,
+                                  const b2_sssp_opts* opts, b2_stream stream, b2_stats* stats) {
+  return run_sssp(g, kModeDelta, source, d_dist, d_pred, opts, (cudaStream_t)stream, stats, true);
 }
 
 extern "C" b2_status b2_graph_trace(b2_graph g, b2_trace_entry* entries, int32_t capacity, int32_t* count) {

@@ -310,3 +310,24 @@ def test_bucket_fusion_is_schedule_only(b2, orc, cuda, fusion):
         dr, _, sr = g.sssp(1, method="delta", delta=delta, fusion_threshold=0, max_iters=3)
         assert np.array_equal(_np(dk), _np(dr)) and sk["converged"] == sr["converged"]
         g.close()
+
+
+@pytest.mark.parametrize("weight", ["u32", "f32"])
+def test_adds_adaptive_width_exact(b2, orc, cuda, weight):
+    """ADDS schedule: bucket width adapted at window boundaries (re-based
+    windows); distances must stay exact and predecessors a shortest-path tree."""
+    for hg in (b2.gen_rmat(13, 16, seed=41), b2.gen_grid(100, 90, 0.02, seed=42), b2.gen_er(5000, 40000, 1, 200, 43)):
+        g = _graph(b2, hg, weight)
+        w = hg.weights if weight == "u32" else hg.fweights
+        deg = np.diff(hg.rowptr)
+        src = int(np.argmax(deg))
+        ref = orc.dijkstra(hg.rowptr, hg.colind, w, src)
+        for delta in (0.0, 1.0 if weight == "u32" else 1e-4):
+            d, p, st = g.sssp(src, method="adds", delta=delta, pred=True)
+            got = _dist_u32(d) if weight == "u32" else _np(d)
+            assert np.array_equal(got, ref), (delta, int(np.sum(got != ref)))
+            assert orc.validate_spt(hg.rowptr, hg.colind, w, src, got, _np(p)) == 0
+            assert st["converged"] == 1
+            if delta:
+                assert st["delta_updates"] > 0 and st["delta_final"] > delta
+        g.close()
