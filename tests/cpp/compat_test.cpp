@@ -1,0 +1,252 @@
+// Drives libb200sssp through the reference's C++ surface (b200sssp/compat.hpp),
+// the way the reference's own drivers do: known answers from
+// HIP_kernel/bellman_ford/tests/test_correctness.cpp, random-graph checks
+// against a CPU Dijkstra as in
+// HIP_kernel/delta_stepping/testing/verify_bf_delta_vs_dijkstra.cpp and
+// Charlotte_oneshot/test_sssp_hip.cpp, and the reference's error conventions.
+// Prints one line per check; exit code 0 only if every check passes.
+#include <cmath>
+#include <cstdio>
+#include <functional>
+#include <limits>
+#include <queue>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "b200sssp/compat.hpp"
+
+static int failures = 0;
+static void check(bool ok, const std::string& what) {
+  std::printf("[%s] %s\n", ok ? "PASS" : "FAIL", what.c_str());
+  if (!ok) ++failures;
+}
+static const float I = std::numeric_limits<float>::infinity();
+
+static bool close_enough(float a, float b) {   // test_correctness.cpp:123-131
+  if (std::isinf(a) || std::isinf(b)) return std::isinf(a) && std::isinf(b);
+  return std::fabs(a - b) <= 1e-4f * (1.0f + std::fabs(a) + std::fabs(b));
+}
+
+// float Dijkstra over outgoing adjacency
+static std::vector<float> dijkstra(int n, const std::vector<int>& rp, const std::vector<int>& ci,
+                                   const std::vector<float>& w, int src) {
+  std::vector<float> d(n, I);
+  using P = std::pair<float, int>;
+  std::priority_queue<P, std::vector<P>, std::greater<P>> q;
+  d[src] = 0.0f;
+  q.push({0.0f, src});
+  while (!q.empty()) {
+    auto [du, u] = q.top();
+    q.pop();
+    if (du != d[u]) continue;
+    for (int e = rp[u]; e < rp[u + 1]; ++e) {
+      const float nd = du + w[e];
+      if (nd < d[ci[e]]) { d[ci[e]] = nd; q.push({nd, ci[e]}); }
+    }
+  }
+  return d;
+}
+
+static int callbacks = 0;
+static void count_cb(const BellmanFordCsrProgress&, void* ud) { ++*static_cast<int*>(ud); }
+
+int main() {
+  // ---- dense BF known answers (test_correctness.cpp:382-418)
+  {
+    std::vector<float> diamond = {I, I, I, I, 2, I, I, I, 5, 1, I, I, I, 4, 1, I};
+    auto r = bellman_ford_minplus_hip(diamond, 4, 0);
+    const float exp[4] = {0, 2, 3, 4};
+    bool ok = r.dist.size() == 4 && r.converged;
+    for (int i = 0; i < 4 && ok; ++i) ok = close_enough(r.dist[i], exp[i]);
+    check(ok, "dense BF flattened_diamond_positive");
+    std::vector<float> neg = {I, I, I, I, 2, 6, I, I, -2, I, 7, 8, I, I, I, I, 5, -3, I, 7, I, -4, 9, I, I};
+    r = bellman_ford_minplus_hip(neg, 5, 0);
+    const float expn[5] = {0, 2, 7, 4, -2};
+    ok = true;
+    for (int i = 0; i < 5 && ok; ++i) ok = close_enough(r.dist[i], expn[i]);
+    check(ok, "dense BF flattened_negative_edges_no_cycle");
+    r = bellman_ford_minplus_hip(std::vector<float>{I}, 1, 0);
+    check(r.dist.size() == 1 && r.dist[0] == 0.0f && r.iterations_used == 0, "dense BF single_vertex");
+    bool threw = false;
+    try { bellman_ford_minplus_hip(diamond, 4, 7); } catch (const std::invalid_argument&) { threw = true; }
+    check(threw, "dense BF source outside graph -> invalid_argument");
+  }
+
+  // ---- random incoming CSR: chain + deg random edges, w in [1,16] (verify_bf_delta_vs_dijkstra.cpp:144-201)
+  const int n = 3000, deg = 8;
+  std::mt19937 rng(1234);
+  std::uniform_int_distribution<int> pick(0, n - 1);
+  std::uniform_real_distribution<float> wd(1.0f, 16.0f);
+  std::vector<std::vector<std::pair<int, float>>> out(n);
+  for (int u = 0; u + 1 < n; ++u) out[u].push_back({u + 1, 1.0f});
+  for (int u = 0; u < n; ++u)
+    for (int k = 0; k < deg; ++k) out[u].push_back({pick(rng), wd(rng)});
+  std::vector<int> orp(n + 1, 0), oci;
+  std::vector<float> ow;
+  for (int u = 0; u < n; ++u) {
+    for (auto& e : out[u]) { oci.push_back(e.first); ow.push_back(e.second); }
+    orp[u + 1] = (int)oci.size();
+  }
+  // incoming CSR (rows = destinations)
+  HostCsrF32 in;
+  in.rows = in.cols = n;
+  std::vector<std::vector<std::pair<int, float>>> inc(n);
+  for (int u = 0; u < n; ++u)
+    for (auto& e : out[u]) inc[e.first].push_back({u, e.second});
+  in.rowptr.push_back(0);
+  for (int v = 0; v < n; ++v) {
+    for (auto& e : inc[v]) { in.colind.push_back(e.first); in.values.push_back(e.second); }
+    in.rowptr.push_back((minplus_sparse::Offset)in.colind.size());
+  }
+  in.nnz = (minplus_sparse::Offset)in.colind.size();
+  const std::vector<float> ref = dijkstra(n, orp, oci, ow, 0);
+  auto agree = [&](const std::vector<float>& d) {   // abs 1e-3 or rel 1e-5 (verify_bf_delta_vs_dijkstra.cpp:26-27)
+    if (d.size() != ref.size()) return false;
+    for (int i = 0; i < n; ++i) {
+      if (std::isinf(ref[i]) != std::isinf(d[i])) return false;
+      if (!std::isinf(ref[i]) && std::fabs(ref[i] - d[i]) > std::max(1e-3f, 1e-5f * std::fabs(ref[i]))) return false;
+    }
+    return true;
+  };
+  callbacks = 0;
+  int cbn = 0;
+  auto bf = bellman_ford_minplus_hip_csr(in, 0, -1, nullptr, count_cb, &cbn);
+  check(agree(bf.dist) && bf.converged && cbn == bf.iterations_used, "CSR BF (checked) vs Dijkstra, callbacks");
+  auto nc = bellman_ford_minplus_hip_csr_no_checks(in, 0, 50);
+  check(agree(nc.dist) && nc.iterations_used == 50, "CSR BF no_checks runs exactly max_iters");
+  auto vc = bellman_ford_minplus_hip_csr_var_checks(in, 0, -1, 7);
+  check(agree(vc.dist) && vc.converged && vc.iterations_used % 7 == 0 && vc.iterations_used >= bf.iterations_used &&
+            vc.iterations_used < bf.iterations_used + 7,
+        "CSR BF var_checks converges on a multiple of the interval");
+  auto ds = delta_stepping_minplus_hip_csr(in, 0, 4.0f, -1);
+  check(agree(ds.dist) && ds.converged, "delta-stepping (delta 4) vs Dijkstra");
+  auto ds2 = delta_stepping_hip_csr(in, 0, 4.0f, 3);
+  check(ds2.iterations_used == 3 && !ds2.converged, "delta-stepping max_iters cut");
+  bool threw = false;
+  try { delta_stepping_minplus_hip_csr(in, 0, -1.0f, -1); } catch (const std::invalid_argument&) { threw = true; }
+  check(threw, "delta-stepping bad delta -> invalid_argument");
+  threw = false;
+  try { bellman_ford_minplus_hip_csr(in, n + 5, -1); } catch (const std::out_of_range&) { threw = true; }
+  check(threw, "CSR BF bad source -> out_of_range");
+
+  // ---- oneshot surface on outgoing CSR
+  CsrGraph g;
+  g.num_nodes = n;
+  g.num_edges = (int)oci.size();
+  g.row_offsets = orp;
+  g.col_indices = oci;
+  g.weights = ow;
+  auto a = adds_sssp_hip(g, 0);
+  check(agree(a.dist) && a.converged && a.final_delta > 0, "adds_sssp_hip vs Dijkstra");
+  auto b = bellman_ford_sssp_hip(g, 0);
+  check(agree(b.dist) && b.converged && !b.has_negative_cycle, "bellman_ford_sssp_hip vs Dijkstra");
+
+  // ---- hip_adds::sssp, uint32 weights, device CSR
+  {
+    std::vector<uint32_t> rp32(orp.begin(), orp.end()), ci32(oci.begin(), oci.end()), w32(ow.size());
+    for (size_t e = 0; e < ow.size(); ++e) w32[e] = (uint32_t)std::lround(ow[e]);
+    std::vector<float> wf(w32.begin(), w32.end());
+    const std::vector<float> refu = dijkstra(n, orp, oci, wf, 0);
+    uint32_t *drp, *dci, *dw, *dd;
+    cudaMalloc(&drp, rp32.size() * 4);
+    cudaMalloc(&dci, ci32.size() * 4);
+    cudaMalloc(&dw, w32.size() * 4);
+    cudaMalloc(&dd, (size_t)n * 4);
+    cudaMemcpy(drp, rp32.data(), rp32.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dci, ci32.data(), ci32.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dw, w32.data(), w32.size() * 4, cudaMemcpyHostToDevice);
+    hip_adds::DeviceCsrGraph<uint32_t> dg;
+    dg.num_vertices = n;
+    dg.num_edges = (uint32_t)ci32.size();
+    dg.row_offsets = drp;
+    dg.col_indices = dci;
+    dg.weights = dw;
+    hip_adds::RunStats rs;
+    auto st = hip_adds::sssp(dg, 0, dd, &rs);
+    std::vector<uint32_t> hd(n);
+    cudaMemcpy(hd.data(), dd, (size_t)n * 4, cudaMemcpyDeviceToHost);
+    bool ok = st == hip_adds::Status::Success && rs.edge_relaxations > 0;
+    for (int i = 0; i < n && ok; ++i) ok = std::isinf(refu[i]) ? hd[i] == 0xFFFFFFFFu : (float)hd[i] == refu[i];
+    check(ok, std::string("hip_adds::sssp uint32 exact (") + hip_adds::status_string(st) + ")");
+    check(hip_adds::sssp(dg, n + 1, dd) == hip_adds::Status::InvalidArgument, "hip_adds::sssp bad source");
+    cudaFree(drp); cudaFree(dci); cudaFree(dw); cudaFree(dd);
+  }
+
+  // ---- min-plus GEMM and SpGEMM
+  {
+    const int M = 37, K = 53, N = 29;
+    std::vector<float> A(M * K), B(K * N), C(M * N);
+    std::uniform_real_distribution<float> u01(0.0f, 1.0f);
+    for (auto& x : A) x = u01(rng) < 0.5f ? I : u01(rng);
+    for (auto& x : B) x = u01(rng) < 0.5f ? I : u01(rng);
+    float *dA, *dB, *dC;
+    cudaMalloc(&dA, A.size() * 4); cudaMalloc(&dB, B.size() * 4); cudaMalloc(&dC, C.size() * 4);
+    cudaMemcpy(dA, A.data(), A.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, B.data(), B.size() * 4, cudaMemcpyHostToDevice);
+    cudaError_t e = minplus_gemm_f32(dA, dB, dC, M, N, K, K, N, N);
+    cudaDeviceSynchronize();
+    cudaMemcpy(C.data(), dC, C.size() * 4, cudaMemcpyDeviceToHost);
+    bool ok = e == cudaSuccess;
+    for (int i = 0; i < M && ok; ++i)
+      for (int j = 0; j < N && ok; ++j) {
+        float acc = I;
+        for (int k = 0; k < K; ++k) { const float c = A[i * K + k] + B[k * N + j]; acc = c < acc ? c : acc; }
+        ok = acc == C[i * N + j];
+      }
+    check(ok, "minplus_gemm_f32 vs naive");
+    check(minplus_gemm_f32(dA, dB, dC, M, N, K, K - 1, N, N) == cudaErrorInvalidValue, "minplus_gemm_f32 lda < K");
+    cudaFree(dA); cudaFree(dB); cudaFree(dC);
+
+    // SpGEMM: A = B = the random outgoing graph's first 200 rows/cols restricted
+    const int m = 200;
+    std::vector<minplus_sparse::Offset> rp(1, 0);
+    std::vector<int> ci;
+    std::vector<float> vv;
+    for (int u = 0; u < m; ++u) {
+      for (int e = orp[u]; e < orp[u + 1]; ++e)
+        if (oci[e] < m) { ci.push_back(oci[e]); vv.push_back(ow[e]); }
+      rp.push_back((minplus_sparse::Offset)ci.size());
+    }
+    minplus_sparse::Offset* drp;
+    int* dci;
+    float* dv;
+    cudaMalloc(&drp, rp.size() * 8); cudaMalloc(&dci, ci.size() * 4); cudaMalloc(&dv, vv.size() * 4);
+    cudaMemcpy(drp, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dci, ci.data(), ci.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dv, vv.data(), vv.size() * 4, cudaMemcpyHostToDevice);
+    minplus_sparse::DeviceCsrF32 S{m, m, (long long)ci.size(), drp, dci, dv};
+    minplus_sparse::Offset* crp = nullptr;
+    minplus_sparse::Index* cci = nullptr;
+    float* cv = nullptr;
+    minplus_sparse::Offset nnz = 0;
+    e = minplus_sparse::minplus_spgemm_csr_f32_tuned<512, 64>(S, S, &crp, &cci, &cv, &nnz);
+    std::vector<minplus_sparse::Offset> hrp(m + 1);
+    std::vector<int> hci(nnz);
+    std::vector<float> hv(nnz);
+    cudaMemcpy(hrp.data(), crp, (m + 1) * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hci.data(), cci, nnz * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hv.data(), cv, nnz * 4, cudaMemcpyDeviceToHost);
+    ok = e == cudaSuccess;
+    for (int i = 0; i < m && ok; ++i) {
+      std::vector<float> row(m, I);
+      for (minplus_sparse::Offset p = rp[i]; p < rp[i + 1]; ++p)
+        for (minplus_sparse::Offset q = rp[ci[p]]; q < rp[ci[p] + 1]; ++q) {
+          const float c = vv[p] + vv[q];
+          if (c < row[ci[q]]) row[ci[q]] = c;
+        }
+      minplus_sparse::Offset pos = hrp[i];
+      for (int j = 0; j < m && ok; ++j)
+        if (!std::isinf(row[j])) { ok = pos < hrp[i + 1] && hci[pos] == j && hv[pos] == row[j]; ++pos; }
+      ok = ok && pos == hrp[i + 1];
+    }
+    check(ok, "minplus_spgemm_csr_f32_tuned<512,64> vs naive (sorted rows)");
+    cudaFree(crp); cudaFree(cci); cudaFree(cv); cudaFree(drp); cudaFree(dci); cudaFree(dv);
+  }
+
+  std::printf("%s: %d failure(s)\n", failures ? "FAILED" : "ALL PASSED", failures);
+  return failures ? 1 : 0;
+}
