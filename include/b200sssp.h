@@ -55,7 +55,8 @@ typedef enum b2_status {
   B2_NOT_SUPPORTED = 8,    /* valid request outside this build's limits */
   B2_INVALID_INDEX = 9,    /* CSR column index out of range */
   B2_INVALID_ROWPTR = 10,  /* CSR row pointer not monotone / out of range */
-  B2_INVALID_WEIGHT = 11   /* negative / NaN weight where the method forbids it */
+  B2_INVALID_WEIGHT = 11,  /* negative / NaN weight where the method forbids it */
+  B2_CANCELLED = 12        /* serving: the query was cancelled before it ran */
 } b2_status;
 
 typedef void* b2_stream; /* cudaStream_t */
@@ -114,7 +115,9 @@ typedef struct b2_sssp_opts {
   int32_t max_iters;        /* BF: rounds (<0: n-1).  delta: buckets (<0: unbounded). */
   int32_t bf_check;         /* b2_bf_check */
   int32_t check_interval;   /* for B2_BF_VAR_CHECKS */
-  int32_t policy;           /* 0: fixed delta (opts.delta or the Near-Far heuristic); 1: learned */
+  int32_t policy;           /* 0: fixed delta (opts.delta or the Near-Far heuristic);
+                               1: learned (b2_policy_activate); overrides delta,
+                               light_heavy and a zero fusion_threshold */
   double delta;             /* bucket width; <=0 selects the Near-Far heuristic */
   double delta_scale;       /* Near-Far constant C in delta = C * mean_w / mean_deg (16) */
   uint32_t hub_degree;      /* vertices with out-degree >= this are split into edge chunks */
@@ -157,7 +160,8 @@ typedef struct b2_stats {
   uint32_t local_subphases; /* delta/ADDS: sub-phases run by one block under bucket fusion */
   uint32_t delta_updates;   /* ADDS: bucket-width changes */
   double delta_final;       /* ADDS: bucket width at the end (delta: = delta_used) */
-  uint32_t reserved[2];
+  uint32_t policy_used;     /* 1: the learned policy chose delta / fusion / light-heavy */
+  uint32_t reserved1;
 } b2_stats;
 
 /* ---- library ---------------------------------------------------------- */
@@ -236,6 +240,134 @@ b2_status b2_minplus_spgemm_f32(const b2_csr* A, const b2_csr* B, int64_t** dC_r
 b2_status b2_minplus_spgemm_i32(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr,
                                 int32_t** dC_colind, int32_t** dC_values, int64_t* hC_nnz,
                                 b2_stream stream);
+
+/* ---- learned schedule policy -------------------------------------------
+ * No counterpart in the reference (it picks delta with the Near-Far rule,
+ * Charlotte_oneshot/sssp_hip.cpp:59-81, which stays the fallback).
+ * Graph features (24 floats) -> MLP 24-64-64-3 (ReLU; BF16 weights, FP32
+ * accumulation; 5955 parameters in the order W1[64x24] b1 W2[64x64] b2
+ * W3[3x64] b3) -> y0 = log2(delta / Near-Far delta) (clamped to [-4, 6]),
+ * y1 > 0: bucket fusion on (threshold 1024), y2 > 0: light/heavy split on.
+ * Features are standardized with the policy's mean/std before the MLP.
+ * Solves with opts.policy = 1 use the active policy; without one they run the
+ * fixed Near-Far schedule (stats.policy_used = 0).  Distances never depend on
+ * the policy. */
+typedef struct b2_policy_s* b2_policy;
+int32_t b2_policy_param_count(void);
+b2_status b2_policy_create(uint64_t seed, b2_policy* out);
+b2_status b2_policy_destroy(b2_policy p);
+/* params: 5955 floats; mu, sigma: 24 floats each (both NULL: unchanged). */
+b2_status b2_policy_set_params(b2_policy p, const float* params, const float* mu, const float* sigma);
+b2_status b2_policy_get_params(b2_policy p, float* params, float* mu, float* sigma);
+/* X: B x 24 raw features; Y: B x 3 outputs. */
+b2_status b2_policy_forward(b2_policy p, const float* X, int32_t B, float* Y);
+/* Gradient of the mean loss (y0-t0)^2 + BCE(y1,t1) + BCE(y2,t2) over the
+ * batch at the current weights; grad: 5955 floats (nullable). */
+b2_status b2_policy_gradient(b2_policy p, const float* X, const float* T, int32_t B, float* grad,
+                             float* loss);
+/* Full-batch AdamW (decoupled weight decay) for `epochs` steps; the first
+ * call also fixes mu/sigma from X. */
+b2_status b2_policy_train(b2_policy p, const float* X, const float* T, int32_t B, int32_t epochs,
+                          float lr, float weight_decay, float* loss_out);
+/* Make p the policy of opts.policy = 1 solves (NULL: none). */
+b2_status b2_policy_activate(b2_policy p);
+/* The 24 schedule features of g (cached on the handle). */
+b2_status b2_graph_features(b2_graph g, float* features);
+
+/* ---- batched serving ----------------------------------------------------
+ * No counterpart in the reference (it answers one query per launch
+ * sequence).  A server holds resident graphs (b2_graph handles that must
+ * outlive it), a device arena of hbm_budget_bytes, and a few CUDA streams.
+ * Submitted single-source queries wait in FIFO order until their arena slot
+ * fits in the budget (b2_server_slot_bytes; a query that can never fit is
+ * refused with B2_OUT_OF_MEMORY at submit), then run in batch launches where
+ * one thread block solves one query alone (delta-stepping, block barriers
+ * only).  Every query owns its slot: results do not depend on what else runs.
+ * out_dist / out_pred must be device memory or page-locked host memory
+ * (cudaHostAlloc / cudaHostRegister); the block writes the result there
+ * directly and a query completes on its own, not with its batch.  Graphs
+ * with negative weights are refused (B2_INVALID_WEIGHT).  Calls on one
+ * server are serialized internally. */
+typedef struct b2_server_s* b2_server;
+typedef struct b2_server_opts {
+  size_t hbm_budget_bytes;  /* device arena (default 1 GiB) */
+  int32_t max_batch;        /* queries per batch launch (default 1024) */
+  int32_t lanes;            /* streams with one batch in flight each (default 4) */
+  int32_t max_inflight;     /* completion records (default 8192) */
+  int32_t blocks_per_sm;    /* 0: occupancy limit */
+  double timeout_ms;        /* per-query device budget (default 20000) */
+  double delta_scale;       /* Near-Far constant for each graph's bucket width (16) */
+  int32_t reserved[4];
+} b2_server_opts;
+typedef struct b2_completion {
+  uint64_t ticket;
+  int32_t status;           /* B2_SUCCESS, B2_TIMEOUT, B2_CANCELLED, ... */
+  int32_t graph_id;
+  uint32_t source;
+  uint32_t phases;
+  uint64_t edges_scanned;
+  uint64_t reached;
+  uint64_t reached_edges;
+  double latency_us;        /* submit -> result in the caller's buffer, observed by the host */
+} b2_completion;
+typedef struct b2_server_info_t {
+  int32_t graphs;
+  uint32_t blocks;          /* resident blocks of one batch launch */
+  int64_t pending;
+  int64_t running;
+  int64_t completed_unpolled;
+  size_t arena_bytes;
+  size_t arena_used;
+} b2_server_info_t;
+void b2_server_opts_default(b2_server_opts* opts);
+b2_status b2_server_create(const b2_server_opts* opts, b2_server* out);
+b2_status b2_server_destroy(b2_server s);
+b2_status b2_server_add_graph(b2_server s, b2_graph g, int32_t* graph_id);
+/* Arena bytes one query on an n-vertex graph holds while it runs. */
+size_t b2_server_slot_bytes(int64_t n, int32_t with_pred);
+b2_status b2_server_submit(b2_server s, int32_t graph_id, uint32_t source, void* out_dist,
+                           int32_t* out_pred, uint64_t* ticket);
+/* A pending query completes with B2_CANCELLED; a running one is never
+ * interrupted (B2_NOT_SUPPORTED). */
+b2_status b2_server_cancel(b2_server s, uint64_t ticket);
+/* Admit and launch what fits, collect finished queries; wait_all = 1 keeps
+ * going until nothing is pending or running. */
+b2_status b2_server_progress(b2_server s, int32_t wait_all);
+b2_status b2_server_poll(b2_server s, b2_completion* out, int32_t capacity, int32_t* count);
+b2_status b2_server_info(b2_server s, b2_server_info_t* info);
+
+/* Built-in load generator over the server's graphs. */
+typedef struct b2_load_opts {
+  int64_t queries;
+  double rate_qps;          /* Poisson arrival rate; <= 0: every query arrives at t = 0 */
+  uint64_t seed;
+  int32_t mode;             /* 0: this server; 1: one query at a time with b2_sssp_delta
+                               on the whole GPU plus a device-to-host copy (baseline) */
+  int32_t with_pred;
+  size_t host_result_bytes; /* page-locked result pool (default 1 GiB); back-pressure when full */
+  const int32_t* graph_ids; /* queries pick uniformly among these (NULL: all graphs) */
+  int32_t n_graph_ids;
+  int32_t reserved0;
+  uint64_t* checksums;      /* nullable [queries]: 64-bit hash of each result's distance words */
+  int32_t* query_graph;     /* nullable [queries]: graph of each query */
+  uint32_t* query_source;   /* nullable [queries]: source of each query */
+  int32_t reserved[4];
+} b2_load_opts;
+typedef struct b2_load_report {
+  int64_t completed;
+  int64_t failed;
+  double elapsed_s;         /* first arrival -> last result in host memory */
+  double qps;
+  double p50_us;            /* latency: scheduled arrival -> result in host memory */
+  double p99_us;
+  double mean_us;
+  double max_us;
+  double gteps;             /* sum of reached out-edges / elapsed */
+  uint64_t reached_edges;
+  double reserved[4];
+} b2_load_report;
+void b2_load_opts_default(b2_load_opts* opts);
+b2_status b2_server_run_load(b2_server s, const b2_load_opts* opts, b2_load_report* report);
 
 /* ---- synthetic graphs (host memory, deterministic, multi-threaded) ----- */
 typedef struct b2_host_csr {

@@ -230,3 +230,64 @@ def delta_bucket_count(dist: np.ndarray, delta, weight: str) -> int:
     b = np.floor(d * inv).astype(np.float64)
     b = np.clip(b, 0, float(0x3fffffff - 1))
     return int(np.unique(b).shape[0])
+
+
+# ---- schedule-policy MLP in FP64 (no reference counterpart) ------------------
+# Layout of the 5955 parameters: W1[64x24] b1[64] W2[64x64] b2[64] W3[3x64] b3[3].
+def bf16_round(x: np.ndarray) -> np.ndarray:
+    """float32 -> nearest bfloat16 (ties to even), returned as float32."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def _mlp_unpack(params):
+    p = np.asarray(params, np.float64)
+    o = 0
+    out = []
+    for shape in ((64, 24), (64,), (64, 64), (64,), (3, 64), (3,)):
+        k = int(np.prod(shape))
+        out.append(p[o:o + k].reshape(shape))
+        o += k
+    assert o == 5955 == p.size
+    return out
+
+
+def mlp_forward(params, Xn):
+    """Outputs (B x 3) for standardized features Xn, FP64 throughout."""
+    W1, b1, W2, b2, W3, b3 = _mlp_unpack(params)
+    h1 = np.maximum(Xn @ W1.T + b1, 0.0)
+    h2 = np.maximum(h1 @ W2.T + b2, 0.0)
+    return h2 @ W3.T + b3
+
+
+def mlp_loss_grad(params, Xn, T):
+    """Mean loss (y0-t0)^2 + BCE-with-logits(y1,t1) + BCE-with-logits(y2,t2)
+    and its gradient with respect to the 5955 parameters, FP64."""
+    W1, b1, W2, b2, W3, b3 = _mlp_unpack(params)
+    Xn = np.asarray(Xn, np.float64)
+    T = np.asarray(T, np.float64)
+    B = Xn.shape[0]
+    a1 = Xn @ W1.T + b1
+    h1 = np.maximum(a1, 0.0)
+    a2 = h1 @ W2.T + b2
+    h2 = np.maximum(a2, 0.0)
+    y = h2 @ W3.T + b3
+    e0 = y[:, 0] - T[:, 0]
+    z = y[:, 1:]
+    t = T[:, 1:]
+    loss = e0 ** 2 + (np.maximum(z, 0) - z * t + np.log1p(np.exp(-np.abs(z)))).sum(1)
+    dy = np.empty_like(y)
+    dy[:, 0] = 2.0 * e0
+    dy[:, 1:] = 1.0 / (1.0 + np.exp(-z)) - t
+    dy /= B
+    gW3 = dy.T @ h2
+    gb3 = dy.sum(0)
+    dh2 = (dy @ W3) * (a2 > 0)
+    gW2 = dh2.T @ h1
+    gb2 = dh2.sum(0)
+    dh1 = (dh2 @ W2) * (a1 > 0)
+    gW1 = dh1.T @ Xn
+    gb1 = dh1.sum(0)
+    g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3])
+    return float(loss.mean()), g

@@ -26,7 +26,7 @@ class B2Error(RuntimeError):
 
 # ---- enums -----------------------------------------------------------------
 SUCCESS, INVALID_ARGUMENT, CUDA_ERROR, OUT_OF_MEMORY, POOL_EXHAUSTED, BUCKET_OVERFLOW, \
-    DEVICE_ERROR, TIMEOUT, NOT_SUPPORTED, INVALID_INDEX, INVALID_ROWPTR, INVALID_WEIGHT = range(12)
+    DEVICE_ERROR, TIMEOUT, NOT_SUPPORTED, INVALID_INDEX, INVALID_ROWPTR, INVALID_WEIGHT, CANCELLED = range(13)
 W_U32, W_F32 = 0, 1
 INCOMING, OUTGOING = 0, 1
 BF_CHECKED, BF_NO_CHECKS, BF_VAR_CHECKS = 0, 1, 2
@@ -68,7 +68,7 @@ class Stats(C.Structure):
                 ("delta_used", C.c_double), ("kernel_ms", C.c_float), ("device_error", C.c_uint32),
                 ("grid_blocks", C.c_uint32), ("first_unchanged", C.c_uint32),
                 ("local_subphases", C.c_uint32), ("delta_updates", C.c_uint32),
-                ("delta_final", C.c_double), ("reserved", C.c_uint32 * 2)]
+                ("delta_final", C.c_double), ("policy_used", C.c_uint32), ("reserved", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -107,6 +107,29 @@ _SIGS = {
                                         C.POINTER(_P), C.POINTER(C.c_int64), _P]),
     "b2_minplus_spgemm_i32": (C.c_int, [C.POINTER(CSR), C.POINTER(CSR), C.POINTER(_P), C.POINTER(_P),
                                         C.POINTER(_P), C.POINTER(C.c_int64), _P]),
+    "b2_policy_param_count": (C.c_int32, []),
+    "b2_policy_create": (C.c_int, [C.c_uint64, C.POINTER(_P)]),
+    "b2_policy_destroy": (C.c_int, [_P]),
+    "b2_policy_set_params": (C.c_int, [_P, _P, _P, _P]),
+    "b2_policy_get_params": (C.c_int, [_P, _P, _P, _P]),
+    "b2_policy_forward": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "b2_policy_gradient": (C.c_int, [_P, _P, _P, C.c_int32, _P, C.POINTER(C.c_float)]),
+    "b2_policy_train": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float,
+                                  C.POINTER(C.c_float)]),
+    "b2_policy_activate": (C.c_int, [_P]),
+    "b2_graph_features": (C.c_int, [_P, _P]),
+    "b2_server_opts_default": (None, [_P]),
+    "b2_server_create": (C.c_int, [_P, C.POINTER(_P)]),
+    "b2_server_destroy": (C.c_int, [_P]),
+    "b2_server_add_graph": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
+    "b2_server_slot_bytes": (C.c_size_t, [C.c_int64, C.c_int32]),
+    "b2_server_submit": (C.c_int, [_P, C.c_int32, C.c_uint32, _P, _P, C.POINTER(C.c_uint64)]),
+    "b2_server_cancel": (C.c_int, [_P, C.c_uint64]),
+    "b2_server_progress": (C.c_int, [_P, C.c_int32]),
+    "b2_server_poll": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
+    "b2_server_info": (C.c_int, [_P, _P]),
+    "b2_load_opts_default": (None, [_P]),
+    "b2_server_run_load": (C.c_int, [_P, _P, _P]),
     "b2_gen_er": (C.c_int, [C.c_int64, C.c_int64, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(HostCSR)]),
     "b2_gen_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint32,
                               C.c_uint32, C.c_uint64, C.POINTER(HostCSR)]),

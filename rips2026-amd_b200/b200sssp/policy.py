@@ -1,0 +1,372 @@
+"""Learned schedule policy: graph features -> MLP -> (delta, fusion, light/heavy).
+
+No counterpart in the reference, which picks delta with the Near-Far rule
+(Charlotte_oneshot/sssp_hip.cpp:59-81, hip_adds_sssp.cpp:1080-1127); that rule
+stays the fallback whenever no policy is active.
+
+The MLP (24 -> 64 -> 64 -> 3, ReLU, BF16 weights with FP32 accumulation) and
+its training run in the library's own CUDA kernels (b2_policy_* in
+include/b200sssp.h).  This module adds:
+
+* ``Policy``: create / forward / gradient / train / activate;
+* weight files: ``.npz`` with ``format_version`` (``save_weights`` /
+  ``load_weights``, pure numpy);
+* the label generator: a sweep of 16 log-spaced delta multipliers x fusion
+  on/off x light/heavy on/off with the delta-stepping kernel, timed on the
+  device, whose fastest configuration is the training target;
+* ``train_default``: builds a set of synthetic graphs (ER, RMAT, perturbed
+  grids; uniform and lognormal weights), labels them, trains, and writes
+  ``policy_weights.npz`` next to this file.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+N_FEATURES = 24
+N_OUTPUTS = 3
+N_PARAMS = 5955
+FORMAT_VERSION = 1
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "policy_weights.npz")
+FEATURE_NAMES = [
+    "log2_n", "log2_m", "avg_degree", "log2_1p_max_degree",
+    "deg_q25", "deg_q50", "deg_q75", "deg_q90", "deg_q99", "zero_degree_frac",
+    "w_q10", "w_q25", "w_q50", "w_q75", "w_q90", "log2_mean_w", "w_cv", "log2_1p_hop_depth",
+    "log2_nearfar_delta", "light_frac", "is_float", "depth_capped", "w_q99", "log2_1p_avg_degree"]
+OUTPUT_NAMES = ["log2_delta_mult", "fusion_logit", "light_heavy_logit"]
+# delta multipliers of the label sweep: 2^(k/2), k = -5 .. 10 (16 log-spaced values)
+SWEEP_LOG2 = [k / 2.0 for k in range(-5, 11)]
+LOG2_MULT_RANGE = (-4.0, 6.0)     # the library clamps y0 to this range
+FUSION_ON = 1024
+
+
+def _fp(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+# ---- weight files (numpy only) ---------------------------------------------
+def save_weights(path: str, params, mu, sigma, **meta) -> None:
+    params = np.asarray(params, np.float32).reshape(-1)
+    mu = np.asarray(mu, np.float32).reshape(-1)
+    sigma = np.asarray(sigma, np.float32).reshape(-1)
+    if params.size != N_PARAMS or mu.size != N_FEATURES or sigma.size != N_FEATURES:
+        raise ValueError("policy weights: wrong shapes")
+    extra = {k: np.asarray(v) for k, v in meta.items()}
+    np.savez(path, format_version=np.int32(FORMAT_VERSION), params=params, mu=mu, sigma=sigma,
+             feature_names=np.array(FEATURE_NAMES), output_names=np.array(OUTPUT_NAMES), **extra)
+
+
+def load_weights(path: str = DEFAULT_WEIGHTS) -> dict:
+    with np.load(path, allow_pickle=False) as z:
+        ver = int(z["format_version"])
+        if ver != FORMAT_VERSION:
+            raise ValueError(f"policy weights {path}: format_version {ver}, expected {FORMAT_VERSION}")
+        out = {k: z[k] for k in z.files}
+    if out["params"].size != N_PARAMS or out["mu"].size != N_FEATURES or out["sigma"].size != N_FEATURES:
+        raise ValueError(f"policy weights {path}: wrong shapes")
+    if list(out["feature_names"]) != FEATURE_NAMES:
+        raise ValueError(f"policy weights {path}: feature list differs from this library's")
+    return out
+
+
+# ---- the device policy -----------------------------------------------------
+class Policy:
+    """One MLP on the current device (FP32 master + BF16 working weights)."""
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        check(lib().b2_policy_create(C.c_uint64(seed), C.byref(h)), "policy_create")
+        self._h = h
+
+    @classmethod
+    def from_file(cls, path: str = DEFAULT_WEIGHTS) -> "Policy":
+        w = load_weights(path)
+        p = cls(0)
+        p.set_params(w["params"], w["mu"], w["sigma"])
+        return p
+
+    def params(self):
+        P = np.zeros(N_PARAMS, np.float32)
+        mu = np.zeros(N_FEATURES, np.float32)
+        sg = np.zeros(N_FEATURES, np.float32)
+        check(lib().b2_policy_get_params(self._h, _fp(P), _fp(mu), _fp(sg)), "policy_get_params")
+        return P, mu, sg
+
+    def set_params(self, params, mu=None, sigma=None) -> None:
+        P = np.ascontiguousarray(params, np.float32)
+        if P.size != N_PARAMS:
+            raise ValueError("params must hold 5955 floats")
+        if mu is not None:
+            mu = np.ascontiguousarray(mu, np.float32)
+            sigma = np.ascontiguousarray(sigma, np.float32)
+            check(lib().b2_policy_set_params(self._h, _fp(P), _fp(mu), _fp(sigma)), "policy_set_params")
+        else:
+            check(lib().b2_policy_set_params(self._h, _fp(P), None, None), "policy_set_params")
+
+    def save(self, path: str, **meta) -> None:
+        P, mu, sg = self.params()
+        save_weights(path, P, mu, sg, **meta)
+
+    def forward(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, N_FEATURES)
+        Y = np.zeros((X.shape[0], N_OUTPUTS), np.float32)
+        check(lib().b2_policy_forward(self._h, _fp(X), X.shape[0], _fp(Y)), "policy_forward")
+        return Y
+
+    def gradient(self, X, T):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, N_FEATURES)
+        T = np.ascontiguousarray(T, np.float32).reshape(-1, N_OUTPUTS)
+        G = np.zeros(N_PARAMS, np.float32)
+        loss = C.c_float()
+        check(lib().b2_policy_gradient(self._h, _fp(X), _fp(T), X.shape[0], _fp(G), C.byref(loss)),
+              "policy_gradient")
+        return G, float(loss.value)
+
+    def train(self, X, T, epochs: int = 2000, lr: float = 3e-3, weight_decay: float = 0.0) -> float:
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, N_FEATURES)
+        T = np.ascontiguousarray(T, np.float32).reshape(-1, N_OUTPUTS)
+        loss = C.c_float()
+        check(lib().b2_policy_train(self._h, _fp(X), _fp(T), X.shape[0], epochs, C.c_float(lr),
+                                    C.c_float(weight_decay), C.byref(loss)), "policy_train")
+        return float(loss.value)
+
+    def activate(self) -> None:
+        check(lib().b2_policy_activate(self._h), "policy_activate")
+
+    @staticmethod
+    def deactivate() -> None:
+        check(lib().b2_policy_activate(None), "policy_activate")
+
+    def decide(self, features) -> dict:
+        y = self.forward(np.asarray(features, np.float32).reshape(1, -1))[0]
+        return {"delta_mult": float(2.0 ** np.clip(y[0], *LOG2_MULT_RANGE)), "fusion": bool(y[1] > 0),
+                "light_heavy": bool(y[2] > 0)}
+
+    def close(self) -> None:
+        if self._h:
+            lib().b2_policy_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def graph_features(g) -> np.ndarray:
+    f = np.zeros(N_FEATURES, np.float32)
+    check(lib().b2_graph_features(g._h, _fp(f)), "graph_features")
+    return f
+
+
+_active: Policy | None = None
+
+
+def activate_default(path: str = DEFAULT_WEIGHTS) -> Policy:
+    """Load the shipped weights and make them the policy of policy=1 solves."""
+    global _active
+    if _active is None:
+        _active = Policy.from_file(path)
+    _active.activate()
+    return _active
+
+
+# ---- label generation ------------------------------------------------------
+def sweep(g, sources, method: str = "delta", reps: int = 1) -> dict:
+    """Time the schedule grid on g; returns {(log2_mult, fusion, lh): ms}.
+
+    Device time of the persistent launches (stats.kernel_ms) summed over the
+    sources; one untimed warm-up solve per configuration.  For integer weights
+    multipliers that floor to the same delta are timed once.
+    """
+    torch = __import__("torch")
+    nf = g.delta_heuristic()
+    out = {}
+    seen = {}
+    dist = torch.empty(g.n, dtype=torch.float32 if g.weight == "f32" else torch.int32, device="cuda")
+    for lm in SWEEP_LOG2:
+        delta = nf * 2.0 ** lm
+        if g.weight == "u32":
+            delta = max(1.0, math.floor(delta))
+        for fu in (0, 1):
+            for lh in (0, 1):
+                key = (delta, fu, lh)
+                if key in seen:
+                    out[(lm, fu, lh)] = seen[key]
+                    continue
+                kw = dict(delta=delta, fusion_threshold=FUSION_ON if fu else 0, light_heavy=lh)
+                g.sssp(int(sources[0]), method=method, out=dist, **kw)
+                ms = 0.0
+                for _ in range(reps):
+                    for s in sources:
+                        _, _, st = g.sssp(int(s), method=method, out=dist, **kw)
+                        ms += st["kernel_ms"]
+                seen[key] = ms
+                out[(lm, fu, lh)] = ms
+    return out
+
+
+def label_from_sweep(times: dict, tol: float = 0.02):
+    """Target (log2 mult, fusion, lh) of the fastest configuration; among
+    configurations within `tol` of the best the one nearest the Near-Far delta
+    wins (labels stay stable under timing noise)."""
+    best = min(times.values())
+    near = [k for k, v in times.items() if v <= best * (1.0 + tol)]
+    k = min(near, key=lambda c: (abs(c[0]), c[1], -c[2]))
+    return np.array([k[0], float(k[1]), float(k[2])], np.float32), best
+
+
+# ---- synthetic training graphs ----------------------------------------------
+def _weights(rng, m, kind, wtype):
+    if kind == "uniform":
+        hi = int(rng.choice([16, 255, 4096, 1 << 16, 1 << 20]))
+        w = rng.integers(1, hi + 1, m).astype(np.float64)
+    else:
+        sig = float(rng.uniform(0.5, 2.0))
+        w = np.exp(rng.normal(np.log(1000.0), sig, m))
+    if wtype == "u32":
+        return np.clip(np.rint(w), 1, 2 ** 31 - 1).astype(np.uint32)
+    return (w / w.max()).astype(np.float32)
+
+
+def training_graph(i: int, max_scale: int = 23, min_scale: int = 16):
+    """Deterministic graph #i of the training family (host arrays): ER, RMAT
+    (a in [0.45, 0.6]) and perturbed grids; 2^min_scale .. 2^max_scale
+    vertices; uniform or lognormal weights, uint32 or float."""
+    from . import gen_er, gen_grid, gen_rmat
+    rng = np.random.default_rng(1000 + i)
+    fam = ["er", "rmat", "grid"][i % 3]
+    wtype = "u32" if (i // 3) % 4 != 3 else "f32"
+    wkind = "uniform" if rng.uniform() < 0.5 else "lognormal"
+    sc = int(rng.integers(min_scale, max_scale + 1))
+    deg = int(rng.choice([4, 8, 16, 32] if sc <= 20 else [4, 8, 16]))
+    if fam == "er":
+        hg = gen_er(1 << sc, deg << sc, 1, 2, seed=i)
+    elif fam == "rmat":
+        a = float(rng.uniform(0.45, 0.6))
+        bc = (1.0 - a) / 3.0
+        hg = gen_rmat(sc, deg, a, bc, bc, 1, 2, seed=i)
+    else:
+        side = int(2 ** rng.uniform(7, (sc + 1) / 2.0))
+        hg = gen_grid(side, side, float(rng.choice([0.0, 0.01, 0.05])), 5.0, 1.0, seed=i)
+    if fam == "grid" and wkind == "lognormal":
+        w = hg.weights if wtype == "u32" else hg.fweights     # the generator's own lognormal law
+    else:
+        w = _weights(rng, hg.m, wkind, wtype)
+    desc = {"family": fam, "n": hg.n, "m": hg.m, "weights": wkind, "wtype": wtype}
+    return hg, w, wtype, desc
+
+
+def times_array(times: dict) -> np.ndarray:
+    """Sweep dict -> [16 multipliers, fusion, light/heavy] array of ms."""
+    A = np.zeros((len(SWEEP_LOG2), 2, 2))
+    for (lm, fu, lh), v in times.items():
+        A[SWEEP_LOG2.index(lm), fu, lh] = v
+    return A
+
+
+def build_dataset(count: int, max_scale: int = 23, n_sources: int = 3, min_scale: int = 16, log=print):
+    """Features X, labels T, full sweep tables and descriptions of `count` graphs."""
+    from . import Graph
+    X, T, TT, info = [], [], [], []
+    for i in range(count):
+        hg, w, wtype, desc = training_graph(i, max_scale, min_scale)
+        g = Graph.from_arrays(hg.rowptr, hg.colind, w, weight=wtype)
+        rng = np.random.default_rng(i)
+        cand = np.nonzero(np.diff(hg.rowptr) > 0)[0]        # sources with out-edges
+        srcs = rng.choice(cand, size=min(n_sources, cand.size), replace=False) if cand.size else [0]
+        del hg, w, cand
+        t0 = time.time()
+        X.append(graph_features(g))
+        times = sweep(g, srcs)
+        y, best = label_from_sweep(times)
+        base = times[(0.0, 0, 1)]
+        T.append(y)
+        TT.append(times_array(times))
+        desc.update(best_ms=best, fixed_ms=base, gain=base / best, label=y.tolist())
+        info.append(desc)
+        log(f"[{i}] {desc} sweep {time.time() - t0:.1f}s")
+        g.close()
+    return np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info
+
+
+def save_dataset(path: str, X, T, TT, info) -> None:
+    import json
+    np.savez(path, format_version=np.int32(FORMAT_VERSION), X=X, T=T, times=TT,
+             sweep_log2=np.array(SWEEP_LOG2), info=np.array(json.dumps(info)))
+
+
+def load_dataset(path: str):
+    import json
+    with np.load(path, allow_pickle=False) as z:
+        return z["X"], z["T"], z["times"], json.loads(str(z["info"]))
+
+
+def train_on(X, T, epochs: int = 3000, lr: float = 3e-3, weight_decay: float = 1e-3, seed: int = 7,
+             out: str | None = DEFAULT_WEIGHTS, **meta) -> "Policy":
+    p = Policy(seed=seed)
+    loss = p.train(X, T, epochs=epochs, lr=lr, weight_decay=weight_decay)
+    if out:
+        p.save(out, n_graphs=np.int32(len(X)), final_loss=np.float32(loss), epochs=np.int32(epochs),
+               lr=np.float32(lr), weight_decay=np.float32(weight_decay), train_X=X, train_T=T, **meta)
+    return p
+
+
+def train_default(count: int = 200, max_scale: int = 23, epochs: int = 3000, lr: float = 3e-3,
+                  weight_decay: float = 1e-3, out: str = DEFAULT_WEIGHTS, dataset_out: str | None = None,
+                  log=print):
+    X, T, TT, info = build_dataset(count, max_scale, log=log)
+    if dataset_out:
+        save_dataset(dataset_out, X, T, TT, info)
+    p = train_on(X, T, epochs, lr, weight_decay, out=out, max_scale=np.int32(max_scale))
+    log(f"trained on {count} graphs -> {out}")
+    return p, X, T, TT, info
+
+
+def compare(g, sources, method: str = "delta", reps: int = 3) -> dict:
+    """Fixed Near-Far schedule vs the active learned policy on g: device time
+    over `sources` (best of `reps`), with the distances of both compared word
+    for word.  Returns times, the speed-up and the policy's choice."""
+    torch = __import__("torch")
+    dt = torch.float32 if g.weight == "f32" else torch.int32
+    res = {}
+    dists = {}
+    for pol in (0, 1):
+        buf = [torch.empty(g.n, dtype=dt, device="cuda") for _ in sources]
+        g.sssp(int(sources[0]), method=method, out=buf[0], policy=pol)      # warm-up (features, light counts)
+        best = float("inf")
+        for _ in range(reps):
+            ms = 0.0
+            for s, b in zip(sources, buf):
+                _, _, st = g.sssp(int(s), method=method, out=b, policy=pol)
+                ms += st["kernel_ms"]
+            best = min(best, ms)
+        res[pol] = (best, st)
+        dists[pol] = [b.view(torch.int32).cpu() for b in buf]
+    same = all(bool(torch.equal(a, b)) for a, b in zip(dists[0], dists[1]))
+    st1 = res[1][1]
+    return {"fixed_ms": res[0][0], "learned_ms": res[1][0], "speedup": res[0][0] / res[1][0],
+            "identical": same, "policy_used": st1["policy_used"], "delta_fixed": res[0][1]["delta_used"],
+            "delta_learned": st1["delta_used"], "local_subphases": st1["local_subphases"]}
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="label synthetic graphs by schedule sweeps and train the policy")
+    ap.add_argument("--graphs", type=int, default=200)
+    ap.add_argument("--max-scale", type=int, default=23)
+    ap.add_argument("--epochs", type=int, default=3000)
+    ap.add_argument("--weight-decay", type=float, default=1e-3)
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--dataset-out", default=None)
+    a = ap.parse_args()
+    train_default(a.graphs, a.max_scale, a.epochs, weight_decay=a.weight_decay, out=a.out,
+                  dataset_out=a.dataset_out)

@@ -19,6 +19,7 @@ extern "C" const char* b2_status_string(b2_status s) {
     case B2_INVALID_INDEX: return "CSR column index out of range";
     case B2_INVALID_ROWPTR: return "CSR row pointer invalid";
     case B2_INVALID_WEIGHT: return "edge weight not allowed for this method";
+    case B2_CANCELLED: return "query cancelled";
   }
   return "unknown status";
 }

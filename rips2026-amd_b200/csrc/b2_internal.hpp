@@ -118,6 +118,7 @@ struct Control {
   uint32_t stamp_ctr;      // next dedup stamp (manager and local loop)
   uint32_t local_q;        // LOCAL phase: queue holding the next frontier
   uint32_t local_iters;    // LOCAL phase: sub-phases run inside it
+  uint32_t fusion_off;     // a LOCAL sub-phase scanned too many edges: no more fusion this solve
   uint32_t local_total;    // sub-phases run by all LOCAL phases
   uint32_t far_min_key;    // adaptive mode: min distance key that landed in the far pile
   uint32_t far_min_key_next;
@@ -177,12 +178,21 @@ struct b2_graph_s {
   bool has_negative = false;
   bool rows_sorted = false;     // each adjacency list ordered by weight
   size_t graph_bytes = 0;
+  float features[24] = {};      // schedule-policy features (computed on first use)
+  bool features_valid = false;
+  uint64_t pol_version = 0;     // policy decision cache: valid when equal to the
+  double pol_mult = 1.0;        // active policy's version
+  int32_t pol_fusion = 0;
+  int32_t pol_lh = 1;
   b2::Workspace ws;
   std::mutex mu;   // one solve at a time per handle
 };
 
 namespace b2 {
 b2_status ensure_workspace(b2_graph g, bool pred);
+// Learned schedule: delta multiplier (x Near-Far delta), fusion and light/heavy
+// choice for g.  B2_NOT_SUPPORTED when no policy is active.
+b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* lh_on);
 b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowptr, const uint2* edges,
                                      int weight_type, b2_graph* out);
 }  // namespace b2

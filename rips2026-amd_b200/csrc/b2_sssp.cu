@@ -833,7 +833,7 @@ __device__ void manager_delta(const Params& P) {
         nx.fq = nn ? r.push_q : kQNone;
         nx.fcount = nn;
         nx.push_q = r.push_q ^ 1u;
-        if (hch == 0 && nn <= P.fusion) nx.kind = kPhaseLocal;
+        if (hch == 0 && nn <= P.fusion && !vld(&c->fusion_off)) nx.kind = kPhaseLocal;
         store_rec(c, nx);
         return;
       }
@@ -883,7 +883,7 @@ __device__ void manager_delta(const Params& P) {
     nx.fq = kQSlot0 + (uint32_t)found;
     nx.fcount = cnts[found];
     nx.push_q = kQNear0;   // both near queues are empty at a bucket boundary
-    if (nx.fcount <= P.fusion) nx.kind = kPhaseLocal;
+    if (nx.fcount <= P.fusion && !vld(&c->fusion_off)) nx.kind = kPhaseLocal;
     store_rec(c, nx);
     return;
   }
@@ -937,20 +937,35 @@ __device__ void manager_delta(const Params& P) {
 // barriers instead of grid barriers; every other block waits at the next grid
 // barrier.  Same relaxation code, same dedup stamps (drawn from the shared
 // stamp counter), no hub splitting.  Exits when the frontier empties or grows
-// past the threshold; the manager continues from local_q.
+// past the threshold; the manager continues from local_q.  A sub-phase that
+// scans more than kLocalEdgesPerVertex * P.fusion edges ends the loop and
+// turns fusion off for the rest of the solve: on graphs whose small frontiers
+// carry many edges one block is slower than the whole grid.
 constexpr uint32_t kMaxLocalIters = 1u << 16;
+constexpr uint32_t kLocalEdgesPerVertex = 8;
 
 template <class W, bool PRED, int MODE>
 __device__ void local_phase(const Params& P, const PhaseRec& R0, Tally& t) {
   __shared__ uint32_t s_l[5];
+  __shared__ unsigned long long s_edges;
   Control* c = P.ctl;
   PhaseRec L = R0;
   const uint32_t w = threadIdx.x >> 5;
   const uint32_t nw = blockDim.x >> 5;
+  const unsigned long long edge_cap = (unsigned long long)P.fusion * kLocalEdgesPerVertex;
+  if (threadIdx.x == 0) s_edges = 0;
+  __syncthreads();
   for (uint32_t iter = 0;; ++iter) {
+    const unsigned long long e0 = t.edges;
     const uint32_t nfc = (L.fcount + 31) / 32;
     for (uint32_t ch = w; ch < nfc; ch += nw) frontier_chunk<W, PRED, MODE>(P, L, ch * 32, t);
     flush_all<MODE>(P, L, t.q, true);
+    {
+      unsigned long long de = t.edges - e0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) de += __shfl_down_sync(0xffffffffu, de, o);
+      if ((threadIdx.x & 31u) == 0 && de) atomicAdd(&s_edges, de);
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -958,7 +973,11 @@ __device__ void local_phase(const Params& P, const PhaseRec& R0, Tally& t) {
       const uint32_t nn = ldcg(&c->near_count[L.push_q & 1]);
       const bool budget = globaltimer_ns() - c->t_start > P.budget_ns;
       if (budget) atomicCAS(&c->error, kErrNone, (uint32_t)kErrTimeout);
-      uint32_t done = (nn == 0 || nn > P.fusion || iter + 1 >= kMaxLocalIters || budget) ? 1u : 0u;
+      const bool heavy_edges = s_edges > edge_cap;
+      s_edges = 0;
+      if (heavy_edges) c->fusion_off = 1u;
+      uint32_t done =
+          (nn == 0 || nn > P.fusion || iter + 1 >= kMaxLocalIters || budget || heavy_edges) ? 1u : 0u;
       if (!done) {
         s_l[0] = L.push_q;
         s_l[1] = nn;
@@ -1215,6 +1234,24 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   if (mode == kModeDelta && g->has_negative) return B2_INVALID_WEIGHT;
   const bool isf = g->weight_type == B2_W_F32;
   const bool pred = d_pred != nullptr;
+  uint32_t policy_used = 0;
+  if (mode == kModeDelta && o.policy == 1) {
+    // learned schedule (computes and caches the graph's features on first use,
+    // which runs solves of its own: before this solve takes the handle lock)
+    double mult = 1.0;
+    int32_t fuse = 0, lh = 1;
+    const b2_status ps = policy_decide(g, &mult, &fuse, &lh);
+    if (ps == B2_SUCCESS) {
+      double nf = 1.0;
+      b2_delta_heuristic(g, o.delta_scale > 0 ? o.delta_scale : 16.0, &nf);
+      o.delta = nf * mult;
+      if (o.fusion_threshold == 0) o.fusion_threshold = fuse ? 1024u : 0u;
+      o.light_heavy = lh;
+      policy_used = 1;
+    } else if (ps != B2_NOT_SUPPORTED) {
+      return ps;
+    }
+  }
   std::lock_guard<std::mutex> lock(g->mu);
   b2_status s = ensure_workspace(g, pred);
   if (s != B2_SUCCESS) return s;
@@ -1280,7 +1317,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       P.adapt = 1;
       P.adapt_cap = (uint32_t)sms * 2u * (uint32_t)kThreads;
-      if (P.fusion == 0 && g->max_degree <= 64) P.fusion = 1024;   // low-degree graphs: fuse tails
+      if (!policy_used && P.fusion == 0 && g->max_degree <= 64) P.fusion = 1024;   // low-degree graphs: fuse tails
     }
     if (o.light_heavy && g->rows_sorted) {
       s = ensure_light_counts(g, isf, P.delta_u, df, st);
@@ -1291,6 +1328,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->delta_used = delta;
+    stats->policy_used = policy_used;
   }
   // zero iterations: only the source is reached (the reference loop never runs)
   if (P.max_iters == 0) {

@@ -1,0 +1,130 @@
+"""GPU: the schedule-policy MLP kernels against the FP64 oracle, training,
+and the learned schedule in the solve path (distances unchanged)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pol(b2, cuda):
+    from b200sssp import policy
+    yield policy
+    policy.Policy.deactivate()
+
+
+def _bf16_params(P, orc):
+    return orc.bf16_round(P).astype(np.float64)
+
+
+def test_forward_matches_fp64_oracle(pol, orc):
+    p = pol.Policy(seed=11)
+    P, mu, sg = p.params()
+    rng = np.random.default_rng(0)
+    X = rng.normal(size=(37, 24)).astype(np.float32)
+    Y = p.forward(X)
+    Xn = (X.astype(np.float64) - mu) / sg
+    ref = orc.mlp_forward(_bf16_params(P, orc), Xn)
+    assert np.allclose(Y, ref, rtol=1e-4, atol=1e-4)     # FP32 accumulation vs FP64
+
+
+def test_gradient_matches_fp64_oracle(pol, orc):
+    p = pol.Policy(seed=5)
+    rng = np.random.default_rng(1)
+    X = rng.normal(size=(50, 24)).astype(np.float32)
+    T = np.c_[rng.normal(size=50), rng.integers(0, 2, (50, 2))].astype(np.float32)
+    # non-trivial normalization
+    P, _, _ = p.params()
+    mu = rng.normal(size=24).astype(np.float32)
+    sg = rng.uniform(0.5, 2.0, 24).astype(np.float32)
+    p.set_params(P, mu, sg)
+    G, loss = p.gradient(X, T)
+    Xn = (X.astype(np.float64) - mu.astype(np.float64)) / sg.astype(np.float64)
+    ref_loss, ref = orc.mlp_loss_grad(_bf16_params(P, orc), Xn, T)
+    assert abs(loss - ref_loss) <= 1e-4 * max(1.0, abs(ref_loss))
+    scale = np.abs(ref).max()
+    assert np.abs(G - ref).max() <= 1e-4 * scale
+    assert np.linalg.norm(G - ref) <= 1e-4 * np.linalg.norm(ref)
+
+
+def test_training_is_deterministic_and_fits(pol):
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=(64, 24)).astype(np.float32)
+    w = rng.normal(size=24)
+    T = np.c_[np.tanh(X @ w / 5) * 3, (X[:, 0] > 0), (X[:, 1] < 0)].astype(np.float32)
+    a, b = pol.Policy(seed=3), pol.Policy(seed=3)
+    la = a.train(X, T, epochs=600, lr=3e-3)
+    lb = b.train(X, T, epochs=600, lr=3e-3)
+    assert la == lb
+    assert np.array_equal(a.params()[0], b.params()[0])
+    _, l0 = pol.Policy(seed=3).gradient(X, T)
+    assert la < 0.25 * l0
+    Y = a.forward(X)
+    assert ((Y[:, 1] > 0) == (T[:, 1] > 0.5)).mean() > 0.9
+
+
+def _raw(d, weight):
+    a = d.cpu().numpy()
+    return a.view(np.uint32) if weight == "u32" else a
+
+
+def _set_constant(p, y):
+    """All weights zero, output biases = y: the policy outputs y for every graph."""
+    P = np.zeros(5955, np.float32)
+    P[-3:] = y
+    p.set_params(P, np.zeros(24, np.float32), np.ones(24, np.float32))
+
+
+@pytest.mark.parametrize("weight", ["u32", "f32"])
+def test_policy_sets_schedule_and_keeps_distances(pol, b2, orc, cuda, weight):
+    hg = b2.gen_rmat(14, 8, seed=4)
+    g = b2.Graph.from_host(hg, weight)
+    nf = g.delta_heuristic()
+    w = hg.weights if weight == "u32" else hg.fweights
+    ref = orc.dijkstra(hg.rowptr, hg.colind, w, 3)
+    p = pol.Policy()
+    _set_constant(p, [2.0, -1.0, 1.0])            # delta x4, fusion off, light/heavy on
+    p.activate()
+    d, _, st = g.sssp(3, policy=1)
+    assert st["policy_used"] == 1
+    want = max(1.0, np.floor(nf * 4.0)) if weight == "u32" else nf * 4.0
+    assert st["delta_used"] == pytest.approx(want, rel=1e-12)
+    assert np.array_equal(_raw(d, weight), ref)
+    _set_constant(p, [-9.0, 1.0, -1.0])            # clamped to /16, fusion on, split off
+    d2, _, st2 = g.sssp(3, policy=1, trace=1)
+    assert st2["policy_used"] == 1
+    want = max(1.0, np.floor(nf / 16.0)) if weight == "u32" else nf / 16.0
+    assert st2["delta_used"] == pytest.approx(want, rel=1e-12)
+    assert not any(t["kind"].endswith("-heavy") for t in g.trace())
+    assert np.array_equal(_raw(d2, weight), ref)
+    pol.Policy.deactivate()                        # no active policy: Near-Far fallback
+    d3, _, st3 = g.sssp(3, policy=1)
+    assert st3["policy_used"] == 0 and st3["delta_used"] == pytest.approx(
+        max(1.0, np.floor(nf)) if weight == "u32" else nf, rel=1e-12)
+    assert np.array_equal(_raw(d3, weight), ref)
+
+
+def test_features_are_cached_and_sane(pol, b2, cuda):
+    hg = b2.gen_grid(64, 64, 0.0, 5.0, 1.0, seed=2)
+    g = b2.Graph.from_host(hg)
+    f = pol.graph_features(g)
+    assert f.shape == (24,) and np.isfinite(f).all()
+    assert f[0] == pytest.approx(12.0)               # log2 n
+    assert f[17] > np.log2(1 + 60)                   # hop depth of a 64 x 64 grid
+    assert np.array_equal(f, pol.graph_features(g))
+
+
+def test_shipped_policy_keeps_distances(pol, b2, orc, cuda):
+    p = pol.activate_default()
+    for hg, weight, s in [(b2.gen_rmat(15, 16, seed=9), "u32", 1), (b2.gen_grid(90, 70, 0.02, seed=3), "f32", 5),
+                          (b2.gen_er(5000, 40000, 1, 1000, seed=1), "u32", 0)]:
+        g = b2.Graph.from_host(hg, weight)
+        w = hg.weights if weight == "u32" else hg.fweights
+        ref = orc.dijkstra(hg.rowptr, hg.colind, w, s)
+        for method in ("delta", "adds"):
+            d, pr, st = g.sssp(s, method=method, policy=1, pred=True)
+            assert st["policy_used"] == 1
+            got = _raw(d, weight)
+            assert np.array_equal(got, ref)
+            assert orc.validate_spt(hg.rowptr, hg.colind, w, s, got, pr.cpu().numpy()) == 0
+    p.deactivate()

@@ -1,0 +1,69 @@
+"""Schedule policy, CPU side: the FP64 MLP oracle against finite differences,
+bfloat16 rounding, and the weight-file format (no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+
+def test_oracle_gradient_matches_finite_differences(orc):
+    rng = np.random.default_rng(3)
+    P = rng.normal(0, 0.2, 5955)
+    X = rng.normal(size=(9, 24))
+    T = np.c_[rng.normal(size=9), rng.integers(0, 2, (9, 2))]
+    _, g = orc.mlp_loss_grad(P, X, T)
+    eps = 1e-6
+    for i in rng.choice(5955, 60, replace=False):
+        Pp, Pm = P.copy(), P.copy()
+        Pp[i] += eps
+        Pm[i] -= eps
+        fd = (orc.mlp_loss_grad(Pp, X, T)[0] - orc.mlp_loss_grad(Pm, X, T)[0]) / (2 * eps)
+        assert abs(fd - g[i]) < 1e-6 * (1 + abs(g[i]))
+    # the forward used by the loss is the same function
+    y = orc.mlp_forward(P, X)
+    assert y.shape == (9, 3)
+
+
+def test_bf16_round_ties_to_even(orc):
+    x = np.array([1.0, 1 + 2 ** -8, 1 + 3 * 2 ** -8, -2.0 - 2 ** -7, 0.0, 1e-40], np.float32)
+    got = orc.bf16_round(x)
+    assert got[:5].tolist() == [1.0, 1.0, 1.015625, -2.0, 0.0]
+
+
+def test_weight_file_round_trip(tmp_path, b2):
+    from b200sssp import policy as pol
+    rng = np.random.default_rng(1)
+    P = rng.normal(size=5955).astype(np.float32)
+    mu = rng.normal(size=24).astype(np.float32)
+    sg = rng.uniform(0.5, 2, 24).astype(np.float32)
+    path = os.path.join(tmp_path, "w.npz")
+    pol.save_weights(path, P, mu, sg, note=np.int32(5))
+    w = pol.load_weights(path)
+    assert np.array_equal(w["params"], P) and np.array_equal(w["mu"], mu) and np.array_equal(w["sigma"], sg)
+    assert int(w["format_version"]) == pol.FORMAT_VERSION and int(w["note"]) == 5
+    bad = dict(w)
+    bad["format_version"] = np.int32(99)
+    np.savez(path, **bad)
+    with pytest.raises(ValueError):
+        pol.load_weights(path)
+    with pytest.raises(ValueError):
+        pol.save_weights(path, P[:-1], mu, sg)
+
+
+def test_shipped_weights_load(b2):
+    from b200sssp import policy as pol
+    w = pol.load_weights()
+    assert w["params"].dtype == np.float32 and np.isfinite(w["params"]).all()
+    assert (w["sigma"] > 0).all()
+    assert int(w["n_graphs"]) > 0
+
+
+def test_label_rule():
+    from b200sssp import policy as pol
+    times = {(lm, fu, lh): 10.0 for lm in pol.SWEEP_LOG2 for fu in (0, 1) for lh in (0, 1)}
+    times[(2.0, 1, 0)] = 5.0
+    times[(-1.0, 0, 1)] = 5.05       # within 2 %: nearer the Near-Far delta, wins
+    y, best = pol.label_from_sweep(times)
+    assert y.tolist() == [-1.0, 0.0, 1.0] and best == 5.0
+    y, _ = pol.label_from_sweep(times, tol=0.0)
+    assert y.tolist() == [2.0, 1.0, 0.0]
