@@ -214,7 +214,7 @@ def sweep(g, sources, method: str = "delta", reps: int = 1) -> dict:
     return out
 
 
-def label_from_sweep(times: dict, tol: float = 0.02):
+def label_from_sweep(times: dict, tol: float = 0.03):
     """Target (log2 mult, fusion, lh) of the fastest configuration; among
     configurations within `tol` of the best the one nearest the Near-Far delta
     wins (labels stay stable under timing noise)."""

@@ -53,6 +53,7 @@ struct MP<float> {
     return r;
   }
   __device__ __forceinline__ static float step1(float acc, float a, float b) { return fminf(acc, a + b); }
+  static constexpr bool kTwoPerMin = true;   // one 3-input min per two pairs
 };
 template <>
 struct MP<int> {
@@ -61,6 +62,7 @@ struct MP<int> {
     return __viaddmin_s32(a1, b1, __viaddmin_s32(a0, b0, acc));
   }
   __device__ __forceinline__ static int step1(int acc, int a, int b) { return __viaddmin_s32(a, b, acc); }
+  static constexpr bool kTwoPerMin = false;  // one fused add+min per pair
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -378,25 +380,47 @@ b2_status apsp(T* D, int N, b2_stream s, int32_t* squarings) {
 }
 
 // ---- ALU peak calibration (roofline denominator for min-plus) -------------
-// Every thread runs `iters` rounds of 16 independent (min,+) pairs on
-// registers; the pair count over the device time is the sustained peak.
+// The GEMM's own instruction mix on registers only: an 8 x 8 accumulator tile
+// per thread updated per k step exactly like mma_tile (int32: one
+// __viaddmin_s32 per pair; fp32: two FADD and one 3-input min per two pairs),
+// with no shared-memory or global traffic.  The A operand of row i at step k
+// is an accumulator of that row (acc[i][(i + k) & 7], a register chosen at
+// compile time), so every sum is a new value and no sum can be folded or
+// shared between pairs; B is 8 (16 for fp32) runtime constants.  The pair
+// count over the device time is the instruction-issue ceiling of the mix.
 template <typename T>
-__global__ void k_calibrate(int iters, T seed, T* sink) {
-  T acc[16];
-  T a = seed + (T)threadIdx.x;
+__global__ void __launch_bounds__(256) k_calibrate(int iters, T seed, T step, T* sink) {
+  T acc[8][8];
+  T b0[8], b1[8];
 #pragma unroll
-  for (int j = 0; j < 16; ++j) acc[j] = MP<T>::init();
-  T b0 = (T)1, b1 = (T)2;
+  for (int j = 0; j < 8; ++j) {
+    b0[j] = step + (T)j;
+    b1[j] = step + (T)(j + 8);
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = seed + (T)(threadIdx.x + 8 * i + j);
   for (int it = 0; it < iters; ++it) {
 #pragma unroll
-    for (int j = 0; j < 16; j += 2) acc[j] = MP<T>::step2(acc[j], a, b0, a, b1);
+    for (int k = 0; k < 8; ++k) {
 #pragma unroll
-    for (int j = 1; j < 16; j += 2) acc[j] = MP<T>::step2(acc[j], b1, a, b0, a);
-    a = a + b0;
+      for (int i = 0; i < 8; ++i) {
+        const T a0 = acc[i][(i + k) & 7];
+        const T a1 = acc[i][(i + k + 3) & 7];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (sizeof(T) == 4 && MP<T>::kTwoPerMin) acc[i][j] = MP<T>::step2(acc[i][j], a0, b0[j], a1, b1[j]);
+          else acc[i][j] = MP<T>::step1(acc[i][j], a0, b0[j]);
+        }
+      }
+    }
   }
-  T r = acc[0];
+  T r = acc[0][0];
 #pragma unroll
-  for (int j = 1; j < 16; ++j) r = r < acc[j] ? r : acc[j];
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r = r < acc[i][j] ? r : acc[i][j];
   if (r == (T)-12345) sink[0] = r;
 }
 
@@ -428,17 +452,17 @@ extern "C" b2_status b2_minplus_calibrate(int32_t is_float, double* pairs_per_se
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int threads = 256, blocks = sms * 8, iters = 1 << 14;
+  const int threads = 256, blocks = sms * 4, iters = 1 << 12;
   void* sink = nullptr;
   B2_CUDA_TRY(cudaMalloc(&sink, 16));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
-  for (int rep = 0; rep < 3; ++rep) {
+  for (int rep = 0; rep < 4; ++rep) {
     cudaEventRecord(e0);
-    if (is_float) k_calibrate<float><<<blocks, threads>>>(iters, 0.5f, (float*)sink);
-    else k_calibrate<int><<<blocks, threads>>>(iters, 3, (int*)sink);
+    if (is_float) k_calibrate<float><<<blocks, threads>>>(iters, 0.5f, 0.25f, (float*)sink);
+    else k_calibrate<int><<<blocks, threads>>>(iters, 3, 1, (int*)sink);
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -450,7 +474,9 @@ extern "C" b2_status b2_minplus_calibrate(int32_t is_float, double* pairs_per_se
   cudaEventDestroy(e1);
   cudaFree(sink);
   if (e != cudaSuccess) return from_cuda(e);
-  *pairs_per_second = (double)blocks * threads * iters * 16.0 / (best * 1e-3);
+  // per thread and iteration: 8 k steps x 64 updates; an fp32 update is two pairs
+  const double pairs = (double)blocks * threads * iters * 8.0 * 64.0 * (is_float ? 2.0 : 1.0);
+  *pairs_per_second = pairs / (best * 1e-3);
   return B2_SUCCESS;
 }
 

@@ -558,7 +558,8 @@ b2_status srv_launch(b2_server s, Lane& ln) {
   std::atomic_thread_fence(std::memory_order_seq_cst);
   const uint32_t nq = (uint32_t)batch.size();
   const uint32_t grid = std::min(nq, s->grid_cap);
-  const unsigned long long budget = (unsigned long long)(std::max(1.0, s->o.timeout_ms) * 1.0e6);
+  // per-query device budget in ns (at least 1 ns: a tiny budget must still time out)
+  const unsigned long long budget = (unsigned long long)std::max(1.0, s->o.timeout_ms * 1.0e6);
   B2_CUDA_TRY(cudaMemsetAsync(ln.d_next, 0, 4, ln.st));
   k_serve<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
   B2_CUDA_TRY(cudaGetLastError());
