@@ -273,11 +273,14 @@ def times_array(times: dict) -> np.ndarray:
     return A
 
 
-def build_dataset(count: int, max_scale: int = 23, n_sources: int = 3, min_scale: int = 16, log=print):
-    """Features X, labels T, full sweep tables and descriptions of `count` graphs."""
+def build_dataset(count: int, max_scale: int = 23, n_sources: int = 3, min_scale: int = 16, log=print,
+                  first: int = 0, checkpoint: str | None = None):
+    """Features X, labels T, full sweep tables and descriptions of graphs
+    first .. first + count - 1 of the training family.  With `checkpoint`
+    the partial dataset is saved after every graph."""
     from . import Graph
     X, T, TT, info = [], [], [], []
-    for i in range(count):
+    for i in range(first, first + count):
         hg, w, wtype, desc = training_graph(i, max_scale, min_scale)
         g = Graph.from_arrays(hg.rowptr, hg.colind, w, weight=wtype)
         rng = np.random.default_rng(i)
@@ -291,10 +294,12 @@ def build_dataset(count: int, max_scale: int = 23, n_sources: int = 3, min_scale
         base = times[(0.0, 0, 1)]
         T.append(y)
         TT.append(times_array(times))
-        desc.update(best_ms=best, fixed_ms=base, gain=base / best, label=y.tolist())
+        desc.update(index=i, best_ms=best, fixed_ms=base, gain=base / best, label=y.tolist())
         info.append(desc)
         log(f"[{i}] {desc} sweep {time.time() - t0:.1f}s")
         g.close()
+        if checkpoint:
+            save_dataset(checkpoint, np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info)
     return np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info
 
 
