@@ -336,6 +336,91 @@ def train_default(count: int = 200, max_scale: int = 23, epochs: int = 3000, lr:
     return p, X, T, TT, info
 
 
+# ---- robust labels, decision cost, cross-validated training ---------------
+FIXED_INDEX = (SWEEP_LOG2.index(0.0), 0, 1)   # Near-Far delta, no fusion, light/heavy on
+
+
+def robust_label(A: np.ndarray, tol: float = 0.03) -> np.ndarray:
+    """Label of one sweep table A[16 multipliers, fusion, light/heavy] (ms).
+
+    Each configuration is scored by its worst time over itself and its two
+    neighbouring multipliers (x 2^-0.5, x 2^0.5) at the same fusion / split
+    setting, so a label sits where the time is flat and a prediction that
+    misses by half a step in log2 costs little.  Among scores within `tol` of
+    the best, the multiplier nearest 1 wins (then fusion off, split on)."""
+    L = A.shape[0]
+    score = np.empty_like(A)
+    for i in range(L):
+        lo, hi = max(0, i - 1), min(L - 1, i + 1)
+        score[i] = A[lo:hi + 1].max(axis=0)
+    best = score.min()
+    cand = [(abs(SWEEP_LOG2[i]), f, -h, i) for i in range(L) for f in (0, 1) for h in (0, 1)
+            if score[i, f, h] <= best * (1.0 + tol)]
+    _, f, nh, i = min(cand)
+    return np.array([SWEEP_LOG2[i], float(f), float(-nh)], np.float32)
+
+
+def decision_index(y) -> tuple[int, int, int]:
+    """Sweep-grid configuration nearest to an MLP output (log2 mult, fusion
+    logit, light/heavy logit), with the library's clamp of the multiplier."""
+    lm = float(np.clip(y[0], *LOG2_MULT_RANGE))
+    i = int(np.argmin([abs(lm - v) for v in SWEEP_LOG2]))
+    return i, int(y[1] > 0), int(y[2] > 0)
+
+
+def decision_speedup(A: np.ndarray, y) -> float:
+    """Fixed-schedule time over the time of the configuration y selects."""
+    return float(A[FIXED_INDEX] / A[decision_index(y)])
+
+
+def cross_validate(X, TT, folds: int = 5, seed: int = 0, epochs: int = 1500, lr: float = 3e-3,
+                   weight_decay: float = 1e-2, tol: float = 0.03) -> dict:
+    """k-fold estimate of the learned schedule's gain on unseen graphs: train
+    on the other folds (GPU kernels), decide for each held-out graph, and read
+    the decision's time off its sweep table.  Returns the geometric-mean
+    speed-up over the fixed schedule, the fraction of graphs slower than
+    fixed, and the oracle (best-in-sweep) speed-up for reference."""
+    X = np.asarray(X, np.float32)
+    T = np.array([robust_label(a, tol) for a in TT], np.float32)
+    idx = np.random.default_rng(seed).permutation(len(X))
+    sp = np.zeros(len(X))
+    for k in range(folds):
+        test = idx[k::folds]
+        train = np.setdiff1d(idx, test)
+        p = Policy(seed=seed + k)
+        p.train(X[train], T[train], epochs=epochs, lr=lr, weight_decay=weight_decay)
+        Y = p.forward(X[test])
+        for j, y in zip(test, Y):
+            sp[j] = decision_speedup(TT[j], y)
+        p.close()
+    best = np.array([a[FIXED_INDEX] / a.min() for a in TT])
+    return {"geo_speedup": float(np.exp(np.log(sp).mean())), "slower_frac": float((sp < 0.99).mean()),
+            "worst": float(sp.min()), "oracle_geo_speedup": float(np.exp(np.log(best).mean())),
+            "per_graph": sp.tolist()}
+
+
+def train_from_dataset(path: str, out: str | None = DEFAULT_WEIGHTS, grid=None, folds: int = 5, seed: int = 7,
+                       log=print):
+    """Relabel a saved sweep dataset with robust_label, pick (epochs, weight
+    decay) by cross-validated speed-up over the fixed schedule, train on all
+    graphs and save the weights with the cross-validation figures."""
+    X, _, TT, info = load_dataset(path)
+    grid = grid or [(800, 1e-2), (1500, 1e-2), (1500, 3e-2), (3000, 3e-3), (3000, 3e-2)]
+    results = []
+    for ep, wd in grid:
+        cv = cross_validate(X, TT, folds=folds, seed=seed, epochs=ep, weight_decay=wd)
+        log(f"cv epochs={ep} wd={wd}: geo speed-up {cv['geo_speedup']:.3f}, slower {cv['slower_frac']:.2f}, "
+            f"worst {cv['worst']:.3f} (best-in-sweep {cv['oracle_geo_speedup']:.3f})")
+        results.append((cv["geo_speedup"], ep, wd, cv))
+    _, ep, wd, cv = max(results, key=lambda r: r[0])
+    T = np.array([robust_label(a) for a in TT], np.float32)
+    p = train_on(X, T, epochs=ep, weight_decay=wd, seed=seed, out=out, cv_geo_speedup=np.float32(cv["geo_speedup"]),
+                 cv_slower_frac=np.float32(cv["slower_frac"]), cv_oracle_geo_speedup=np.float32(cv["oracle_geo_speedup"]),
+                 cv_folds=np.int32(folds))
+    log(f"trained on {len(X)} graphs (epochs={ep}, wd={wd}) -> {out}")
+    return p, cv
+
+
 def compare(g, sources, method: str = "delta", reps: int = 3) -> dict:
     """Fixed Near-Far schedule vs the active learned policy on g: device time
     over `sources` (best of `reps`), with the distances of both compared word
@@ -372,6 +457,10 @@ if __name__ == "__main__":
     ap.add_argument("--weight-decay", type=float, default=1e-3)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--dataset-out", default=None)
+    ap.add_argument("--from-dataset", default=None, help="retrain from a saved sweep dataset (cross-validated)")
     a = ap.parse_args()
-    train_default(a.graphs, a.max_scale, a.epochs, weight_decay=a.weight_decay, out=a.out,
-                  dataset_out=a.dataset_out)
+    if a.from_dataset:
+        train_from_dataset(a.from_dataset, out=a.out)
+    else:
+        train_default(a.graphs, a.max_scale, a.epochs, weight_decay=a.weight_decay, out=a.out,
+                      dataset_out=a.dataset_out)

@@ -9,21 +9,34 @@
 // Unlike the reference (per-row shared-memory hash with a fixed capacity and
 // unsorted output) rows have no size limit and output columns are sorted.
 //
-// Expand-sort-compress:
-//   1. k_row_bound   : candidates per row = sum of |B row k| over A's row;
-//                      validates A's and B's row pointers and A's columns;
-//   2. scan          : candidate offsets (CUB);
-//   3. k_expand      : one warp per row writes (column, value) candidates,
-//                      B rows read as contiguous lane-strided runs;
-//   4. segmented sort: candidates of each row by column (CUB, stable);
-//   5. k_count / scan / k_compress: one warp per row min-reduces runs of
-//                      equal columns and writes the exact-size output.
+// Plan (one pass over the expansion for ordinary rows):
+//   1. k_row_bound : candidates per row (sum of |B row k| over A's row);
+//                    validates A's and B's row pointers and A's columns and
+//                    lists the rows with more than kWarpRowMax candidates;
+//   2. scan        : candidate offsets (CUB) = each row's slot in a scratch
+//                    array sized by the bound;
+//   3. k_rows_warp : one warp per ordinary row gathers its candidates into
+//                    shared memory as 64-bit keys (column << 32 | order-
+//                    preserving value bits), sorts them in registers with a
+//                    bitonic network (32 x P keys, P = 1..16), and writes the
+//                    first key of every column run (= the run's minimum) to
+//                    the row's scratch slot with its count;
+//   4. long rows   : expand-sort-compress over the listed rows only
+//                    (k_expand, CUB segmented sort, k_compress into the same
+//                    scratch slots);
+//   5. scan of the counts (CUB) -> C.rowptr, then k_compact copies every row
+//      from its scratch slot to the exact-size outputs.
+// Scratch arrays come from a library-owned stream-ordered memory pool that
+// keeps up to 4 GiB cached between calls (no cudaMalloc / cudaFree on the
+// critical path after the first call).
 // The int32 twin treats values >= INT32_MAX/2 as absent and drops sums that
 // reach it.
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "b2_common.cuh"
@@ -34,6 +47,9 @@ namespace {
 
 constexpr int32_t kMiss32 = 1073741823;
 constexpr int32_t kDropCol = 0x7fffffff;   // sorts after every real column
+constexpr int kWarpRowMax = 512;           // candidates of a row sorted in one warp's registers
+constexpr int kRowWarps = 8;               // warps per block of k_rows_warp
+constexpr unsigned long long kNoKey = ~0ull;
 
 enum SpStatus : uint32_t { kSpOk = 0, kSpBadIndex = 1, kSpBadRowptr = 2 };
 
@@ -60,9 +76,25 @@ struct SpVal<int32_t> {
   __device__ __forceinline__ static int32_t vmin(int32_t x, int32_t y) { return y < x ? y : x; }
 };
 
+// Order-preserving 32-bit encodings of the values (sorting (column, key)
+// pairs puts each column's minimum first).
+template <typename T>
+struct VKey;
+template <>
+struct VKey<float> {
+  __device__ __forceinline__ static uint32_t enc(float v) { return f32_to_key(v); }
+  __device__ __forceinline__ static float dec(uint32_t k) { return key_to_f32(k); }
+};
+template <>
+struct VKey<int32_t> {
+  __device__ __forceinline__ static uint32_t enc(int32_t v) { return (uint32_t)v ^ 0x80000000u; }
+  __device__ __forceinline__ static int32_t dec(uint32_t k) { return (int32_t)(k ^ 0x80000000u); }
+};
+
 __global__ void k_row_bound(int64_t M, int64_t K, int64_t annz, int64_t bnnz, const int64_t* __restrict__ arp,
                             const int32_t* __restrict__ aci, const int64_t* __restrict__ brp,
-                            unsigned long long* __restrict__ ub, uint32_t* status) {
+                            unsigned long long* __restrict__ ub, uint32_t* status, int64_t* __restrict__ long_rows,
+                            unsigned long long* __restrict__ long_count) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
@@ -87,21 +119,172 @@ __global__ void k_row_bound(int64_t M, int64_t K, int64_t annz, int64_t bnnz, co
       }
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) ub[i] = s;
+    if (lane == 0) {
+      ub[i] = s;
+      if (s > (unsigned long long)kWarpRowMax) long_rows[atomicAdd(long_count, 1ull)] = i;
+    }
   }
 }
 
+// ---- ordinary rows: one warp, registers -----------------------------------
+__device__ __forceinline__ unsigned long long shfl_xor64(unsigned long long x, int m) {
+  const uint32_t lo = __shfl_xor_sync(0xffffffffu, (uint32_t)x, m);
+  const uint32_t hi = __shfl_xor_sync(0xffffffffu, (uint32_t)(x >> 32), m);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+// Sort the row's n <= 32 P staged keys (element e = r * 32 + lane holds
+// key[r]; padding is kNoKey), then write the head of every column run.
+template <typename T, int P>
+__device__ __forceinline__ uint32_t sort_and_emit(const unsigned long long* __restrict__ sk, uint32_t n,
+                                                  int32_t* __restrict__ tcol, T* __restrict__ tval) {
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long key[P];
+#pragma unroll
+  for (int r = 0; r < P; ++r) {
+    const uint32_t e = (uint32_t)r * 32u + lane;
+    key[r] = e < n ? sk[e] : kNoKey;
+  }
+  // bitonic network over 32 P elements, ascending
+#pragma unroll
+  for (int k = 2; k <= 32 * P; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+#pragma unroll
+        for (int r = 0; r < P; ++r) {
+          const int rp = r ^ (j >> 5);
+          if (rp > r) {
+            const bool up = ((r * 32) & k) == 0;
+            const unsigned long long x = key[r], y = key[rp];
+            if ((x > y) == up) {
+              key[r] = y;
+              key[rp] = x;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < P; ++r) {
+          const uint32_t e = (uint32_t)r * 32u + lane;
+          const bool up = (e & (uint32_t)k) == 0;
+          const unsigned long long o = shfl_xor64(key[r], j);
+          const bool lower = (lane & (uint32_t)j) == 0;
+          const bool take_min = lower == up;
+          key[r] = take_min ? (o < key[r] ? o : key[r]) : (o > key[r] ? o : key[r]);
+        }
+      }
+    }
+  }
+  // heads of column runs, in order
+  uint32_t cnt = 0;
+  uint32_t carry = 0xFFFFFFFFu;   // column of element r * 32 - 1
+#pragma unroll
+  for (int r = 0; r < P; ++r) {
+    const uint32_t col = (uint32_t)(key[r] >> 32);
+    uint32_t pc = __shfl_up_sync(0xffffffffu, col, 1);
+    if (lane == 0) pc = carry;
+    const bool head = key[r] != kNoKey && col != pc;
+    const uint32_t b = __ballot_sync(0xffffffffu, head);
+    if (head) {
+      const uint32_t pos = cnt + __popc(b & ((1u << lane) - 1u));
+      tcol[pos] = (int32_t)col;
+      tval[pos] = VKey<T>::dec((uint32_t)key[r]);
+    }
+    cnt += __popc(b);
+    carry = __shfl_sync(0xffffffffu, col, 31);
+  }
+  return cnt;
+}
+
 template <typename T>
-__global__ void k_expand(int64_t M, int64_t N, const int64_t* __restrict__ arp, const int32_t* __restrict__ aci,
-                         const T* __restrict__ av, const int64_t* __restrict__ brp,
+__global__ void __launch_bounds__(kRowWarps * 32)
+    k_rows_warp(int64_t M, int64_t N, const int64_t* __restrict__ arp, const int32_t* __restrict__ aci,
+                const T* __restrict__ av, const int64_t* __restrict__ brp, const int32_t* __restrict__ bci,
+                const T* __restrict__ bv, const unsigned long long* __restrict__ off, int32_t* __restrict__ tcol,
+                T* __restrict__ tval, int64_t* __restrict__ cnt, uint32_t* status) {
+  __shared__ unsigned long long s_keys[kRowWarps][kWarpRowMax];
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long* sk = s_keys[threadIdx.x >> 5];
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = warp; i < M; i += nwarps) {
+    const unsigned long long o0 = off[i], ub = off[i + 1] - o0;
+    if (ub > (unsigned long long)kWarpRowMax) continue;   // long row: expand-sort-compress
+    if (ub == 0) {
+      if (lane == 0) cnt[i] = 0;
+      continue;
+    }
+    // gather: up to 32 A entries at a time; lane t holds entry t's B range
+    uint32_t n = 0;
+    const int64_t a0 = arp[i], a1 = arp[i + 1];
+    for (int64_t pa = a0; pa < a1; pa += 32) {
+      const int64_t p = pa + lane;
+      T a = T(0);
+      int64_t b0 = 0;
+      uint32_t len = 0;
+      if (p < a1) {
+        const int32_t k = aci[p];
+        a = av[p];
+        if (SpVal<T>::present(a)) {
+          b0 = brp[k];
+          len = (uint32_t)(brp[k + 1] - b0);
+        }
+      }
+      const uint32_t incl = warp_incl_scan(len);
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      const uint32_t excl = incl - len;
+      for (uint32_t s0 = 0; s0 < total; s0 += 32) {
+        const uint32_t sl = s0 + lane;
+        // owner: the last lane whose range starts at or before slot sl
+        uint32_t t = 0;
+#pragma unroll
+        for (uint32_t step = 16; step >= 1; step >>= 1) {
+          const uint32_t e = __shfl_sync(0xffffffffu, excl, t + step);
+          if (e <= sl) t += step;
+        }
+        const uint32_t ex_t = __shfl_sync(0xffffffffu, excl, t);
+        const long long b0_t = __shfl_sync(0xffffffffu, (long long)b0, t);
+        const T a_t = __shfl_sync(0xffffffffu, a, t);
+        if (sl < total) {
+          const int64_t q = b0_t + (int64_t)(sl - ex_t);
+          const int32_t j = bci[q];
+          T c = T(0);
+          bool ok = SpVal<T>::combine(a_t, bv[q], c);
+          if (j < 0 || (int64_t)j >= N) {
+            atomicCAS(status, kSpOk, (uint32_t)kSpBadIndex);
+            ok = false;
+          }
+          sk[n + sl] = ok ? (((unsigned long long)(uint32_t)j << 32) | VKey<T>::enc(c)) : kNoKey;
+        }
+      }
+      n += total;
+    }
+    __syncwarp();
+    uint32_t kept;
+    if (n <= 32) kept = sort_and_emit<T, 1>(sk, n, tcol + o0, tval + o0);
+    else if (n <= 64) kept = sort_and_emit<T, 2>(sk, n, tcol + o0, tval + o0);
+    else if (n <= 128) kept = sort_and_emit<T, 4>(sk, n, tcol + o0, tval + o0);
+    else if (n <= 256) kept = sort_and_emit<T, 8>(sk, n, tcol + o0, tval + o0);
+    else kept = sort_and_emit<T, 16>(sk, n, tcol + o0, tval + o0);
+    if (lane == 0) cnt[i] = kept;
+    __syncwarp();
+  }
+}
+
+// ---- long rows: expand-sort-compress over a row list -----------------------
+template <typename T>
+__global__ void k_expand(int64_t L, const int64_t* __restrict__ rows, int64_t N, const int64_t* __restrict__ arp,
+                         const int32_t* __restrict__ aci, const T* __restrict__ av, const int64_t* __restrict__ brp,
                          const int32_t* __restrict__ bci, const T* __restrict__ bv,
                          const unsigned long long* __restrict__ off, int32_t* __restrict__ ccol,
                          T* __restrict__ cval, uint32_t* status) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
-  for (int64_t i = warp; i < M; i += nwarps) {
-    unsigned long long pos = off[i];
+  for (int64_t r = warp; r < L; r += nwarps) {
+    const int64_t i = rows[r];
+    unsigned long long pos = off[r];
     for (int64_t p = arp[i]; p < arp[i + 1]; ++p) {
       const int32_t k = aci[p];
       const T a = av[p];
@@ -124,34 +307,21 @@ __global__ void k_expand(int64_t M, int64_t N, const int64_t* __restrict__ arp, 
   }
 }
 
-// distinct kept columns per row (runs of equal columns in the sorted segment)
-__global__ void k_count(int64_t M, const unsigned long long* __restrict__ off, const int32_t* __restrict__ scol,
-                        int64_t* __restrict__ cnt) {
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const uint32_t lane = threadIdx.x & 31u;
-  for (int64_t i = warp; i < M; i += nwarps) {
-    const unsigned long long b = off[i], e = off[i + 1];
-    long long c = 0;
-    for (unsigned long long q = b + lane; q < e; q += 32) {
-      const int32_t j = scol[q];
-      if (j != kDropCol && (q == b || scol[q - 1] != j)) ++c;
-    }
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-    if (lane == 0) cnt[i] = c;
-  }
-}
-
+// Heads of column runs of each listed row's sorted segment -> the row's
+// scratch slot (tcol / tval at slot[row]) and its count.
 template <typename T>
-__global__ void k_compress(int64_t M, const unsigned long long* __restrict__ off, const int32_t* __restrict__ scol,
-                           const T* __restrict__ sval, const int64_t* __restrict__ crp, int32_t* __restrict__ cci,
-                           T* __restrict__ cv) {
+__global__ void k_compress(int64_t L, const int64_t* __restrict__ rows, const unsigned long long* __restrict__ off,
+                           const int32_t* __restrict__ scol, const T* __restrict__ sval,
+                           const unsigned long long* __restrict__ slot, int32_t* __restrict__ tcol,
+                           T* __restrict__ tval, int64_t* __restrict__ cnt) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
-  for (int64_t i = warp; i < M; i += nwarps) {
-    const unsigned long long b = off[i], e = off[i + 1];
-    int64_t outpos = crp[i];
+  for (int64_t rr = warp; rr < L; rr += nwarps) {
+    const int64_t i = rows[rr];
+    const unsigned long long b = off[rr], e = off[rr + 1];
+    const unsigned long long dst = slot[i];
+    int64_t outpos = 0;
     for (unsigned long long base = b; base < e; base += 32) {
       const unsigned long long q = base + lane;
       const bool in = q < e;
@@ -163,10 +333,35 @@ __global__ void k_compress(int64_t M, const unsigned long long* __restrict__ off
         T m = sval[q];
         for (unsigned long long r = q + 1; r < e && scol[r] == j; ++r) m = SpVal<T>::vmin(m, sval[r]);
         const int64_t w = outpos + __popc(hm & ((1u << lane) - 1u));
-        cci[w] = j;
-        cv[w] = m;
+        tcol[dst + w] = j;
+        tval[dst + w] = m;
       }
       outpos += __popc(hm);
+    }
+    if (lane == 0) cnt[i] = outpos;
+  }
+}
+
+__global__ void k_long_bounds(int64_t L, const int64_t* __restrict__ rows, const unsigned long long* __restrict__ off,
+                              unsigned long long* __restrict__ lub) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < L; r += (int64_t)gridDim.x * blockDim.x)
+    lub[r] = off[rows[r] + 1] - off[rows[r]];
+}
+
+// scratch slots -> exact-size outputs (one warp per row)
+template <typename T>
+__global__ void k_compact(int64_t M, const unsigned long long* __restrict__ slot, const int64_t* __restrict__ crp,
+                          const int32_t* __restrict__ tcol, const T* __restrict__ tval, int32_t* __restrict__ cci,
+                          T* __restrict__ cv) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (int64_t i = warp; i < M; i += nwarps) {
+    const unsigned long long s0 = slot[i];
+    const int64_t c0 = crp[i], c = crp[i + 1] - c0;
+    for (int64_t q = lane; q < c; q += 32) {
+      cci[c0 + q] = tcol[s0 + q];
+      cv[c0 + q] = tval[s0 + q];
     }
   }
 }
@@ -178,11 +373,49 @@ int grid_rows(int64_t rows) {
   return (int)b;
 }
 
+// Library-owned stream-ordered pool for scratch arrays, one per device; it
+// keeps up to kPoolKeep bytes cached after a call returns.
+constexpr uint64_t kPoolKeep = 4ull << 30;
+cudaError_t scratch_pool(cudaMemPool_t* out) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t p;
+  e = cudaMemPoolCreate(&p, &props);
+  if (e != cudaSuccess) return e;
+  uint64_t keep = kPoolKeep;
+  cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[dev] = p;
+  *out = p;
+  return cudaSuccess;
+}
+
+// Scratch array from the pool, released (stream-ordered) on scope exit.
 template <typename T>
 struct DBuf {
   T* p = nullptr;
-  ~DBuf() { if (p) cudaFree(p); }
-  cudaError_t alloc(size_t n) { return cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T)); }
+  cudaStream_t st = nullptr;
+  ~DBuf() { if (p) cudaFreeAsync(p, st); }
+  cudaError_t alloc(size_t n, cudaStream_t s) {
+    st = s;
+    cudaMemPool_t pool;
+    cudaError_t e = scratch_pool(&pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync((void**)&p, std::max<size_t>(n, 1) * sizeof(T), pool, s);
+  }
 };
 
 template <typename T>
@@ -216,61 +449,102 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
     *dC_rowptr = crp;
     return B2_SUCCESS;
   }
-  DBuf<unsigned long long> ub, off;
+  DBuf<unsigned long long> ub, off, lcount;
+  DBuf<int64_t> lrows;
   DBuf<uint32_t> status;
   DBuf<unsigned char> tmp;
-  if (ub.alloc((size_t)M + 1) != cudaSuccess || off.alloc((size_t)M + 1) != cudaSuccess ||
-      status.alloc(1) != cudaSuccess)
+  if (ub.alloc((size_t)M + 1, st) != cudaSuccess || off.alloc((size_t)M + 1, st) != cudaSuccess ||
+      status.alloc(1, st) != cudaSuccess || lrows.alloc((size_t)M, st) != cudaSuccess ||
+      lcount.alloc(1, st) != cudaSuccess)
     return fail(B2_OUT_OF_MEMORY);
   cudaError_t e = cudaMemsetAsync(status.p, 0, 4, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ub.p + M, 0, 8, st);
-  k_row_bound<<<grid_rows(M), 256, 0, st>>>(M, K, A->nnz, B->nnz, arp, A->colind, brp, ub.p, status.p);
-  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemsetAsync(lcount.p, 0, 8, st);
+  if (e == cudaSuccess) {
+    k_row_bound<<<grid_rows(M), 256, 0, st>>>(M, K, A->nnz, B->nnz, arp, A->colind, brp, ub.p, status.p, lrows.p,
+                                              lcount.p);
+    e = cudaGetLastError();
+  }
   size_t tb = 0;
   if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb, ub.p, off.p, M + 1, st);
-  if (e == cudaSuccess) e = tmp.alloc(tb);
+  if (e == cudaSuccess) e = tmp.alloc(tb, st);
   if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp.p, tb, ub.p, off.p, M + 1, st);
-  unsigned long long U = 0;
+  unsigned long long hv[2] = {0, 0};   // total candidates, long rows
   uint32_t hs = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&U, off.p + M, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hv[0], off.p + M, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hv[1], lcount.p, 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, status.p, 4, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return fail(from_cuda(e));
   if (hs == kSpBadIndex) return fail(B2_INVALID_INDEX);
   if (hs == kSpBadRowptr) return fail(B2_INVALID_ROWPTR);
-  if (U > 0x7fffffffull) return fail(B2_NOT_SUPPORTED);   // segmented sort item count is int
-  DBuf<int32_t> col0, col1;
-  DBuf<T> val0, val1;
+  const unsigned long long U = hv[0];
+  const int64_t L = (int64_t)hv[1];
+  DBuf<int32_t> tcol;
+  DBuf<T> tval;
   DBuf<int64_t> cnt;
-  if (col0.alloc(U) != cudaSuccess || col1.alloc(U) != cudaSuccess || val0.alloc(U) != cudaSuccess ||
-      val1.alloc(U) != cudaSuccess || cnt.alloc((size_t)M + 1) != cudaSuccess)
+  if (tcol.alloc(U, st) != cudaSuccess || tval.alloc(U, st) != cudaSuccess ||
+      cnt.alloc((size_t)M + 1, st) != cudaSuccess)
     return fail(B2_OUT_OF_MEMORY);
   if (U > 0) {
-    k_expand<T><<<grid_rows(M), 256, 0, st>>>(M, N, arp, A->colind, (const T*)A->values, brp, B->colind,
-                                              (const T*)B->values, off.p, col0.p, val0.p, status.p);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t want = (M + kRowWarps - 1) / kRowWarps;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 6));
+    k_rows_warp<T><<<blocks, kRowWarps * 32, 0, st>>>(M, N, arp, A->colind, (const T*)A->values, brp, B->colind,
+                                                    (const T*)B->values, off.p, tcol.p, tval.p, cnt.p, status.p);
     e = cudaGetLastError();
-    size_t tb2 = 0;
-    DBuf<unsigned char> tmp2;
-    if (e == cudaSuccess)
-      e = cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb2, col0.p, col1.p, val0.p, val1.p, (int)U, (int)M,
-                                                    off.p, off.p + 1, st);
-    if (e == cudaSuccess) e = tmp2.alloc(tb2);
-    if (e == cudaSuccess)
-      e = cub::DeviceSegmentedSort::StableSortPairs(tmp2.p, tb2, col0.p, col1.p, val0.p, val1.p, (int)U, (int)M,
-                                                    off.p, off.p + 1, st);
-    if (e == cudaSuccess) {
-      k_count<<<grid_rows(M), 256, 0, st>>>(M, off.p, col1.p, cnt.p);
-      e = cudaGetLastError();
-    }
   } else {
     e = cudaMemsetAsync(cnt.p, 0, (size_t)M * sizeof(int64_t), st);
   }
+  // long rows: expand, segmented sort, compress into their scratch slots
+  DBuf<unsigned long long> lub, loff;
+  DBuf<int32_t> col0, col1;
+  DBuf<T> val0, val1;
+  DBuf<unsigned char> tmp2, tmp3;
+  if (e == cudaSuccess && L > 0) {
+    if (lub.alloc((size_t)L + 1, st) != cudaSuccess || loff.alloc((size_t)L + 1, st) != cudaSuccess)
+      return fail(B2_OUT_OF_MEMORY);
+    e = cudaMemsetAsync(lub.p + L, 0, 8, st);
+    if (e == cudaSuccess) {
+      k_long_bounds<<<(int)std::min<int64_t>((L + 255) / 256, 1184), 256, 0, st>>>(L, lrows.p, off.p, lub.p);
+      e = cudaGetLastError();
+    }
+    size_t tb1 = 0;
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb1, lub.p, loff.p, L + 1, st);
+    if (e == cudaSuccess) e = tmp2.alloc(tb1, st);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp2.p, tb1, lub.p, loff.p, L + 1, st);
+    unsigned long long LU = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&LU, loff.p + L, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(from_cuda(e));
+    if (LU > 0x7fffffffull) return fail(B2_NOT_SUPPORTED);   // segmented sort item count is int
+    if (col0.alloc(LU, st) != cudaSuccess || col1.alloc(LU, st) != cudaSuccess || val0.alloc(LU, st) != cudaSuccess ||
+        val1.alloc(LU, st) != cudaSuccess)
+      return fail(B2_OUT_OF_MEMORY);
+    k_expand<T><<<grid_rows(L), 256, 0, st>>>(L, lrows.p, N, arp, A->colind, (const T*)A->values, brp, B->colind,
+                                              (const T*)B->values, loff.p, col0.p, val0.p, status.p);
+    e = cudaGetLastError();
+    size_t tbs = 0;
+    if (e == cudaSuccess)
+      e = cub::DeviceSegmentedSort::StableSortPairs(nullptr, tbs, col0.p, col1.p, val0.p, val1.p, (int)LU, (int)L,
+                                                    loff.p, loff.p + 1, st);
+    if (e == cudaSuccess) e = tmp3.alloc(tbs, st);
+    if (e == cudaSuccess)
+      e = cub::DeviceSegmentedSort::StableSortPairs(tmp3.p, tbs, col0.p, col1.p, val0.p, val1.p, (int)LU, (int)L,
+                                                    loff.p, loff.p + 1, st);
+    if (e == cudaSuccess) {
+      k_compress<T><<<grid_rows(L), 256, 0, st>>>(L, lrows.p, loff.p, col1.p, val1.p, off.p, tcol.p, tval.p, cnt.p);
+      e = cudaGetLastError();
+    }
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(cnt.p + M, 0, 8, st);
-  size_t tb3 = 0;
-  DBuf<unsigned char> tmp3;
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb3, cnt.p, crp, M + 1, st);
-  if (e == cudaSuccess) e = tmp3.alloc(tb3);
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp3.p, tb3, cnt.p, crp, M + 1, st);
+  size_t tb4 = 0;
+  DBuf<unsigned char> tmp4;
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb4, cnt.p, crp, M + 1, st);
+  if (e == cudaSuccess) e = tmp4.alloc(tb4, st);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp4.p, tb4, cnt.p, crp, M + 1, st);
   int64_t nnz = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nnz, crp + M, 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, status.p, 4, cudaMemcpyDeviceToHost, st);
@@ -286,7 +560,7 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
       cudaFree(cci);
       return fail(B2_OUT_OF_MEMORY);
     }
-    k_compress<T><<<grid_rows(M), 256, 0, st>>>(M, off.p, col1.p, val1.p, crp, cci, cv);
+    k_compact<T><<<grid_rows(M), 256, 0, st>>>(M, off.p, crp, tcol.p, tval.p, cci, cv);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {

@@ -83,3 +83,38 @@ def test_spgemm_invalid_inputs(b2, cuda):
     with pytest.raises(b2.B2Error) as e:      # A.cols != B.rows
         b2.minplus_spgemm((rp, good_ci, v, 3), (rp, good_ci, v, 2))
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.int32])
+def test_spgemm_row_sizes_across_sort_widths(b2, orc, cuda, dtype):
+    """Rows whose candidate counts sit on every register-sort width boundary
+    (32 x 1 .. 32 x 16) and just past the one-warp limit (512), where rows
+    switch to expand-sort-compress; columns collide heavily so runs are long."""
+    rng = np.random.default_rng(17)
+    K, N = 700, 97
+    blen = np.where(np.arange(K) < 600, 1, rng.integers(2, 9, K))      # rows 0..599 hold one entry
+    brp = np.concatenate([[0], np.cumsum(blen)]).astype(np.int64)
+    bci = rng.integers(0, N, int(brp[-1])).astype(np.int32)
+    targets = [1, 2, 31, 32, 33, 63, 64, 65, 127, 128, 129, 255, 256, 257, 511, 512, 513, 640, 2000]
+    rows, vals = [], []
+    for t in targets:
+        if t <= 600:
+            cols = rng.permutation(600)[:t]
+        else:
+            cols = np.concatenate([rng.permutation(600), rng.integers(600, K, (t - 600) // 4 + 1)])
+        rows.append(cols.astype(np.int32))
+    arp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int64)
+    aci = np.concatenate(rows)
+    if dtype == np.float32:
+        av = rng.uniform(0, 1, aci.size).astype(np.float32)
+        bv = rng.uniform(0, 1, bci.size).astype(np.float32)
+        av[rng.uniform(size=av.size) < 0.02] = np.inf
+    else:
+        av = rng.integers(1, 1000, aci.size).astype(np.int32)
+        bv = rng.integers(1, 1000, bci.size).astype(np.int32)
+        bv[rng.uniform(size=bv.size) < 0.02] = MISS
+    A, B = (arp, aci, av), (brp, bci, bv)
+    got = _gpu(b2, cuda, A, B, N)
+    ref = orc.minplus_spgemm(A, B, N)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)

@@ -62,8 +62,33 @@ def test_label_rule():
     from b200sssp import policy as pol
     times = {(lm, fu, lh): 10.0 for lm in pol.SWEEP_LOG2 for fu in (0, 1) for lh in (0, 1)}
     times[(2.0, 1, 0)] = 5.0
-    times[(-1.0, 0, 1)] = 5.05       # within 2 %: nearer the Near-Far delta, wins
+    times[(-1.0, 0, 1)] = 5.05       # within 3 %: nearer the Near-Far delta, wins
     y, best = pol.label_from_sweep(times)
     assert y.tolist() == [-1.0, 0.0, 1.0] and best == 5.0
     y, _ = pol.label_from_sweep(times, tol=0.0)
     assert y.tolist() == [2.0, 1.0, 0.0]
+
+
+def test_robust_label_prefers_flat_side():
+    """A sharp minimum next to a cliff loses to a slightly slower flat region;
+    the decision cost reads the chosen configuration off the sweep table."""
+    from b200sssp import policy as pol
+    L = len(pol.SWEEP_LOG2)
+    A = np.full((L, 2, 2), 10.0)
+    i0 = pol.SWEEP_LOG2.index(0.0)
+    A[:, 0, 1] = 10.0
+    A[i0 - 2, 0, 1] = 7.0          # sharp minimum at x 2^-1 ...
+    A[i0 - 3, 0, 1] = 30.0         # ... next to a cliff
+    A[i0 + 2: i0 + 5, 0, 1] = 8.0  # flat region at x 2^1 .. 2^2
+    y = pol.robust_label(A)
+    assert y.tolist() == [1.5, 0.0, 1.0]          # middle of the flat region
+    assert pol.decision_speedup(A, y) == pytest.approx(10.0 / 8.0)
+    assert pol.decision_speedup(A, [-1.0, -3.0, 2.0]) == pytest.approx(10.0 / 7.0)
+    assert pol.decision_index([99.0, 1.0, -1.0]) == (L - 1, 1, 0)   # clamped multiplier
+
+
+def test_shipped_dataset_matches_weights():
+    from b200sssp import policy as pol
+    X, T, TT, info = pol.load_dataset(os.path.join(os.path.dirname(pol.DEFAULT_WEIGHTS), "policy_dataset.npz"))
+    assert X.shape[0] == TT.shape[0] == len(info) > 0
+    assert TT.shape[1:] == (len(pol.SWEEP_LOG2), 2, 2) and np.isfinite(TT).all()
