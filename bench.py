@@ -645,6 +645,7 @@ def workload_serve(args):
     srv = serving.Server(hbm_budget=120 << 30, max_batch=1024)
     for g in graphs:
         srv.add_graph(g)
+        g.sssp(0, collect_reach=1)          # warm the one-at-a-time path: workspace, light counts
     srv.run_load(256, rate_qps=0.0, seed=99, mode="server")                  # warm-up
     rep = srv.run_load(args.queries, rate_qps=args.rate, seed=SEED, mode="server")
     seq = srv.run_load(1024, rate_qps=0.0, seed=SEED, mode="sequential")

@@ -261,7 +261,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   auto fr = [](void* p) { if (p) cudaFree(p); };
   fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
   fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
-  fr(w.ctl);
+  fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   w = Workspace();
   const size_t word = pred ? 8 : 4;
@@ -287,11 +287,12 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   if (e == cudaSuccess) e = al((void**)&w.queues, (5 + (size_t)kRing) * n * 4);
   if (e == cudaSuccess) e = al((void**)&w.hubs, 2 * w.hub_cap * sizeof(HubEntry));
   if (e == cudaSuccess) e = al((void**)&w.ctl, sizeof(Control));
+  if (e == cudaSuccess) e = al((void**)&w.reach, 2 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&w.h_ctl, sizeof(Control));
   if (e != cudaSuccess) {
     fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
     fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
-    fr(w.ctl);
+    fr(w.ctl); fr(w.reach);
     if (w.h_ctl) cudaFreeHost(w.h_ctl);
     w = Workspace();
     return from_cuda(e);
@@ -411,7 +412,7 @@ extern "C" b2_status b2_graph_destroy(b2_graph g) {
   fr(g->rowptr); fr(g->edges); fr(g->in_rowptr32);
   fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
   fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
-  fr(w.ctl);
+  fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   delete g;
   return B2_SUCCESS;

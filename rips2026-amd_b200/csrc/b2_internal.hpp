@@ -158,6 +158,7 @@ struct Workspace {
   size_t hub_cap = 0;
   Control* ctl = nullptr;
   Control* h_ctl = nullptr;   // pinned mirror for the result read-back
+  unsigned long long* reach = nullptr;   // [reached vertices, their out-edges] of the last solve
   uint32_t phase_epoch = 0;
   size_t bytes = 0;
 };

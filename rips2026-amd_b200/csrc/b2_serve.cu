@@ -118,33 +118,47 @@ struct SShared {
   unsigned long long red[3];
 };
 
-// Relax one edge (u's label key -> v); pushes v to the next near queue or the far pile.
+// Relax kSU edges per lane (u's label key -> v): all edge loads are issued
+// first, then all label loads, then the atomics, so one lane keeps kSU
+// independent memory requests in flight; improved vertices go to the next
+// near queue or the far pile (warp-aggregated appends).
+constexpr int kSU = 4;
+
 template <class W, bool PRED>
-__device__ __forceinline__ void relax_edge(const ServeQuery& q, SShared& sh, uint32_t ukey, uint32_t u, uint2 e,
-                                           bool valid, uint32_t next_stamp, uint32_t* qnext) {
+__device__ __forceinline__ void relax_edges(const ServeQuery& q, SShared& sh, const uint32_t (&ukey)[kSU],
+                                            const uint32_t (&u)[kSU], const uint2 (&e)[kSU], const bool (&valid)[kSU],
+                                            uint32_t next_stamp, uint32_t* qnext) {
   using L = SLabel<PRED>;
-  bool to_near = false, to_far = false;
-  uint32_t v = e.x;
-  if (valid) {
-    const uint32_t nd = W::extend(ukey, e.y);
-    typename L::T* lab = (typename L::T*)q.labels;
-    const uint32_t cur_key = L::key(__ldcg(lab + v));
+  typename L::T* lab = (typename L::T*)q.labels;
+  uint32_t nd[kSU], cur[kSU];
+#pragma unroll
+  for (int k = 0; k < kSU; ++k) {
+    nd[k] = valid[k] ? W::extend(ukey[k], e[k].y) : kInfKey;
+    cur[k] = nd[k] != kInfKey ? L::key(__ldcg(lab + e[k].x)) : kInfKey;
+  }
+  bool imp[kSU];
+#pragma unroll
+  for (int k = 0; k < kSU; ++k) {
+    imp[k] = false;
     // with predecessors an equal distance may still lower the predecessor id
-    if (nd != kInfKey && (PRED ? nd <= cur_key : nd < cur_key)) {
-      const typename L::T old = L::atomic_min(lab + v, L::make(nd, u));
-      if (nd < L::key(old)) {
-        if (sbucket<W>(q, nd) <= sh.cur) {
-          to_near = atomicExch(q.stamp + v, next_stamp) != next_stamp;
-        } else {
-          to_far = atomicExch(q.farflag + v, 1u) == 0u;
-        }
-      }
+    if (nd[k] != kInfKey && (PRED ? nd[k] <= cur[k] : nd[k] < cur[k])) {
+      const typename L::T old = L::atomic_min(lab + e[k].x, L::make(nd[k], u[k]));
+      imp[k] = nd[k] < L::key(old);
     }
   }
-  const uint32_t pn = warp_append(&sh.next_count, to_near);
-  if (to_near) qnext[pn] = v;
-  const uint32_t pf = warp_append(&sh.fcount, to_far);
-  if (to_far) q.fa[pf] = v;
+#pragma unroll
+  for (int k = 0; k < kSU; ++k) {
+    bool to_near = false, to_far = false;
+    const uint32_t v = e[k].x;
+    if (imp[k]) {
+      if (sbucket<W>(q, nd[k]) <= sh.cur) to_near = atomicExch(q.stamp + v, next_stamp) != next_stamp;
+      else to_far = atomicExch(q.farflag + v, 1u) == 0u;
+    }
+    const uint32_t pn = warp_append(&sh.next_count, to_near);
+    if (to_near) qnext[pn] = v;
+    const uint32_t pf = warp_append(&sh.fcount, to_far);
+    if (to_far) q.fa[pf] = v;
+  }
 }
 
 // One near phase: warps take 32-vertex chunks of the frontier and walk the
@@ -177,24 +191,29 @@ __device__ void near_phase(const ServeQuery& q, SShared& sh, const uint32_t* qcu
     const uint32_t incl = warp_incl_scan(deg);
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     const uint32_t excl = incl - deg;
-    for (uint32_t e0 = 0; e0 < total; e0 += 32) {
-      const uint32_t e = e0 + lane;
-      // owner: first lane whose inclusive prefix exceeds e
-      uint32_t lo = 0;
+    for (uint32_t e0 = 0; e0 < total; e0 += 32 * kSU) {
+      uint32_t okey[kSU], ou[kSU];
+      uint2 ed[kSU];
+      bool valid[kSU];
 #pragma unroll
-      for (uint32_t s = 16; s > 0; s >>= 1) {
-        const uint32_t pv = __shfl_sync(0xffffffffu, incl, lo + s - 1);
-        if (pv <= e) lo += s;
+      for (int k = 0; k < kSU; ++k) {
+        const uint32_t e = e0 + 32u * k + lane;
+        // owner: first lane whose inclusive prefix exceeds e
+        uint32_t lo = 0;
+#pragma unroll
+        for (uint32_t s = 16; s > 0; s >>= 1) {
+          const uint32_t pv = __shfl_sync(0xffffffffu, incl, lo + s - 1);
+          if (pv <= e) lo += s;
+        }
+        const uint32_t owner = lo > 31 ? 31 : lo;
+        const uint32_t oex = __shfl_sync(0xffffffffu, excl, owner);
+        const uint64_t ost = __shfl_sync(0xffffffffu, start, owner);
+        okey[k] = __shfl_sync(0xffffffffu, ukey, owner);
+        ou[k] = __shfl_sync(0xffffffffu, u, owner);
+        valid[k] = e < total;
+        ed[k] = valid[k] ? __ldcs(q.edges + ost + (e - oex)) : make_uint2(0, 0);
       }
-      const uint32_t owner = lo > 31 ? 31 : lo;
-      const uint32_t oex = __shfl_sync(0xffffffffu, excl, owner);
-      const uint64_t ost = __shfl_sync(0xffffffffu, start, owner);
-      const uint32_t okey = __shfl_sync(0xffffffffu, ukey, owner);
-      const uint32_t ou = __shfl_sync(0xffffffffu, u, owner);
-      const bool valid = e < total;
-      uint2 ed = make_uint2(0, 0);
-      if (valid) ed = __ldcs(q.edges + ost + (e - oex));
-      relax_edge<W, PRED>(q, sh, okey, ou, ed, valid, next_stamp, qnext);
+      relax_edges<W, PRED>(q, sh, okey, ou, ed, valid, next_stamp, qnext);
     }
     edges += deg;
   }
@@ -206,12 +225,19 @@ __device__ void near_phase(const ServeQuery& q, SShared& sh, const uint32_t* qcu
     const uint64_t start = __ldg(q.rowptr + u), end = __ldg(q.rowptr + u + 1);
     const uint64_t len = end - start;
     // every thread of the block runs the same number of iterations (warp_append needs whole warps)
-    for (uint64_t k0 = 0; k0 < len; k0 += kServeThreads) {
-      const uint64_t k = k0 + threadIdx.x;
-      const bool valid = k < len;
-      uint2 ed = make_uint2(0, 0);
-      if (valid) ed = __ldcs(q.edges + start + k);
-      relax_edge<W, PRED>(q, sh, ukey, u, ed, valid, next_stamp, qnext);
+    for (uint64_t k0 = 0; k0 < len; k0 += (uint64_t)kServeThreads * kSU) {
+      uint32_t okey[kSU], ou[kSU];
+      uint2 ed[kSU];
+      bool valid[kSU];
+#pragma unroll
+      for (int j = 0; j < kSU; ++j) {
+        const uint64_t k = k0 + (uint64_t)j * kServeThreads + threadIdx.x;
+        valid[j] = k < len;
+        okey[j] = ukey;
+        ou[j] = u;
+        ed[j] = valid[j] ? __ldcs(q.edges + start + k) : make_uint2(0, 0);
+      }
+      relax_edges<W, PRED>(q, sh, okey, ou, ed, valid, next_stamp, qnext);
     }
     if (threadIdx.x == 0) edges += len;
   }

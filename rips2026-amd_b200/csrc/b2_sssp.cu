@@ -53,7 +53,19 @@ namespace b2 {
 
 enum Mode : int { kModeBF = 0, kModeDelta = 1 };
 constexpr int kThreads = 512;
-constexpr int kUnroll = 4;   // edge slots per lane per step
+#ifndef B2_UNROLL
+#define B2_UNROLL 4
+#endif
+#ifndef B2_HUB_UNROLL
+#define B2_HUB_UNROLL 4
+#endif
+#ifndef B2_HUB_GRAB
+#define B2_HUB_GRAB 4
+#endif
+#ifndef B2_STATIC_NUM   // share of a phase's items dealt round-robin: NUM / 4 (the rest from a counter)
+#define B2_STATIC_NUM 3
+#endif
+constexpr int kUnroll = B2_UNROLL;   // edge slots per lane per step
 
 struct Params {
   uint32_t n;
@@ -455,20 +467,22 @@ __device__ __forceinline__ void hub_chunk(const Params& P, const PhaseRec& R, ui
   phase_range(P, R, v, rlo, rhi, hh);
   const uint64_t e0 = rlo + (uint64_t)h.y * kHubChunk;
   const uint64_t e1 = min(rhi, e0 + kHubChunk);
-  // the whole chunk in one step: kHubChunk / 32 edge loads per lane in flight
-  constexpr int U = (int)(kHubChunk / 32);
-  bool act[U];
-  uint32_t src[U], dsrc[U];
-  uint2 ed[U];
+  // B2_HUB_UNROLL edge loads per lane in flight per step
+  constexpr int U = B2_HUB_UNROLL;
+  for (uint64_t eb = e0; eb < e1; eb += 32 * U) {
+    bool act[U];
+    uint32_t src[U], dsrc[U];
+    uint2 ed[U];
 #pragma unroll
-  for (int q = 0; q < U; ++q) {
-    const uint64_t e = e0 + 32 * q + lane;
-    act[q] = e < e1;
-    src[q] = v;
-    dsrc[q] = du;
-    ed[q] = act[q] ? __ldcs(&P.edges[e]) : make_uint2(0, 0);
+    for (int q = 0; q < U; ++q) {
+      const uint64_t e = eb + 32 * q + lane;
+      act[q] = e < e1;
+      src[q] = v;
+      dsrc[q] = du;
+      ed[q] = act[q] ? __ldcs(&P.edges[e]) : make_uint2(0, 0);
+    }
+    relax_batch<W, PRED, MODE, U>(P, R, act, src, dsrc, ed, t);
   }
-  relax_batch<W, PRED, MODE, U>(P, R, act, src, dsrc, ed, t);
 }
 
 // One frontier chunk: entries [base, base + 32) of the frontier queue.
@@ -566,7 +580,7 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
 // A relaxation phase: hub chunks of the previous phase, then 32-vertex
 // frontier chunks, handed out one at a time from a phase counter so no warp
 // idles while another holds a long tail.
-constexpr uint32_t kHubGrab = 4;   // hub chunks per work item (1024 edges)
+constexpr uint32_t kHubGrab = B2_HUB_GRAB;   // hub chunks per work item
 
 // A relaxation phase: hub chunks of the previous phase, then 32-vertex
 // frontier chunks.  Items are first dealt round-robin to the warps (3/4 of
@@ -580,7 +594,7 @@ __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t items = nhg + nfc;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t rounds = (items * 3 / 4) / nwarps;
+  const uint32_t rounds = (items * B2_STATIC_NUM / 4) / nwarps;
   const uint32_t nstatic = rounds * nwarps;
   Control* c = P.ctl;
   auto run = [&](uint32_t item) {
@@ -1416,16 +1430,14 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   }
   if (ds != B2_SUCCESS) return ds;
   if (stats && o.collect_reach) {
-    unsigned long long* d_r = nullptr;
-    B2_CUDA_TRY(cudaMalloc((void**)&d_r, 16));
-    cudaMemsetAsync(d_r, 0, 16, st);
+    unsigned long long* d_r = w.reach;   // workspace counters: no allocation (a cudaFree would sync the device)
+    B2_CUDA_TRY(cudaMemsetAsync(d_r, 0, 16, st));
     const void* lab = pred ? w.dist_a : d_dist;
     if (pred) k_reach<true><<<1024, 256, 0, st>>>(P.n, g->rowptr, lab, isf, d_r);
     else k_reach<false><<<1024, 256, 0, st>>>(P.n, g->rowptr, lab, isf, d_r);
     unsigned long long hr[2] = {0, 0};
     cudaMemcpyAsync(hr, d_r, 16, cudaMemcpyDeviceToHost, st);
     e = cudaStreamSynchronize(st);
-    cudaFree(d_r);
     if (e != cudaSuccess) return from_cuda(e);
     stats->reached = hr[0];
     stats->reached_edges = hr[1];
