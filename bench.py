@@ -142,6 +142,24 @@ def pick_sources(hg, k: int, seed: int) -> list[int]:
     return out
 
 
+def shard_sources(sources: list[int], rank: int, world: int) -> list[int]:
+    """Replicas: rank r solves sources r, r + world, ... (every rank at least one)."""
+    return sources[rank::world] if world <= len(sources) else [sources[rank % len(sources)]]
+
+
+def reduce_over_ranks(times, counts, device, distributed: bool):
+    """Max over ranks of the timed intervals, sum of the work counts; every
+    rank calls it once, in the same order (one MAX then one SUM all-reduce)."""
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([float(x) for x in times], dtype=torch.float64, device=device)
+    tot = torch.tensor([float(x) for x in counts], dtype=torch.float64, device=device)
+    if distributed:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return tt.tolist(), tot.tolist()
+
+
 def cpu_reference_sample(hg, iterations: int, budget_s: float = 12.0) -> dict:
     """Time the reference's min-plus BF iteration (numpy port) on a row sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -266,7 +284,7 @@ def main():
         return
 
     g = b200sssp.Graph.from_host(hg, "u32")
-    my_sources = sources[rank::world] if world <= NSRC else [sources[rank % NSRC]]
+    my_sources = shard_sources(sources, rank, world)
     stream = torch.cuda.Stream()
     opts = {}
     if args.policy == "learned":
@@ -330,13 +348,8 @@ def main():
     sampler.stop()
 
     # max over ranks
-    tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
-    tot = torch.tensor([float(edges), float(e2e_edges)], dtype=torch.float64, device="cuda")
-    if distributed:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    t_dev, t_e2e = tt.tolist()
-    edges_all, e2e_all = tot.tolist()
+    (t_dev, t_e2e), (edges_all, e2e_all) = reduce_over_ranks([t_dev, t_e2e], [edges, e2e_edges], "cuda",
+                                                             distributed)
 
     if args.trace_out and rank == 0:
         _, _, stt = g.sssp(my_sources[0], method=args.method, out=dist_out, stream=stream, trace=1, **opts)

@@ -665,7 +665,7 @@ extern "C" void b2_server_opts_default(b2_server_opts* o) {
   o->lanes = 4;
   o->max_inflight = 8192;
   o->timeout_ms = 20000.0;
-  o->delta_scale = 16.0;
+  o->delta_scale = 4.0;   // narrower than the full-GPU default: a CTA's phases end with block barriers
   o->blocks_per_sm = 0;
 }
 
@@ -733,7 +733,7 @@ extern "C" b2_status b2_server_add_graph(b2_server s, b2_graph g, int32_t* graph
   G.n = (uint32_t)g->n;
   G.isf = g->weight_type == B2_W_F32;
   double delta = 1.0;
-  b2_delta_heuristic(g, s->o.delta_scale > 0 ? s->o.delta_scale : 16.0, &delta);
+  b2_delta_heuristic(g, s->o.delta_scale > 0 ? s->o.delta_scale : 4.0, &delta);
   if (G.isf) {
     const float df = (float)delta;
     if (!(df > 0.0f) || !std::isfinite(df)) return B2_INVALID_ARGUMENT;
@@ -954,7 +954,7 @@ extern "C" b2_status b2_server_run_load(b2_server s, const b2_load_opts* opts, b
     b2_sssp_opts so;
     b2_sssp_opts_default(&so);
     so.timeout_ms = s->o.timeout_ms;
-    so.delta_scale = s->o.delta_scale;
+    // (the plain solver's own Near-Far delta: this mode is the one-at-a-time baseline)
     so.collect_reach = 1;
     for (int64_t i = 0; i < Q && status == B2_SUCCESS; ++i) {
       const uint64_t due = t0 + (uint64_t)(arrival[i] * 1e9);
