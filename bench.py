@@ -661,6 +661,7 @@ def workload_serve(args):
         g.sssp(0, collect_reach=1)          # warm the one-at-a-time path: workspace, light counts
     srv.run_load(256, rate_qps=0.0, seed=99, mode="server")                  # warm-up
     rep = srv.run_load(args.queries, rate_qps=args.rate, seed=SEED, mode="server")
+    light = srv.run_load(2048, rate_qps=1000.0, seed=SEED + 1, mode="server")      # below capacity
     seq = srv.run_load(1024, rate_qps=0.0, seed=SEED, mode="sequential")
     srv.close()
     return _line("serve_qps", rep["qps"], "queries/s", args, 1e3 / max(rep["qps"], 1e-9), "u32",
@@ -670,6 +671,7 @@ def workload_serve(args):
                       "d2h_bytes_per_step": "distance array of the query's graph"},
                  gpu_launches=None,
                  detail={"p50_us": rep["p50_us"], "p99_us": rep["p99_us"], "server": rep, "sequential": seq,
+                         "light_load_1000qps": light,
                          "speedup_over_sequential_qps": rep["qps"] / max(seq["qps"], 1e-9),
                          "graph_gen_s": t_gen})
 

@@ -177,6 +177,14 @@ b2_status b2_device_copy(void* d_dst, const void* d_src, size_t bytes, b2_stream
 b2_status b2_graph_create(const b2_csr* csr, b2_stream stream, b2_graph* out);
 b2_status b2_graph_destroy(b2_graph g);
 b2_status b2_graph_info_get(b2_graph g, b2_graph_info* info);
+/* Degree order (no reference counterpart): renumber the resident graph's
+ * vertices internally by out-degree, descending, so the few hot vertices of a
+ * skewed graph share cache lines.  Every interface keeps input vertex ids:
+ * sources are mapped in and distances / predecessors scattered back.
+ * b2_graph_create applies it by itself to graphs with >= 2^23 vertices and
+ * max degree >= 64 x mean degree; this call forces it (idempotent). */
+b2_status b2_graph_set_degree_order(b2_graph g, b2_stream stream);
+int32_t b2_graph_degree_ordered(b2_graph g);
 /* Near-Far delta = scale * mean(w > 0) / mean degree (>= 1 for uint32). */
 b2_status b2_delta_heuristic(b2_graph g, double scale, double* delta_out);
 /* Phase trace of the last solve on g that ran with opts.trace = 1. */

@@ -200,6 +200,14 @@ class Graph:
         check(lib().b2_graph_info_get(self._h, C.byref(info)), "graph_info")
         return {k: getattr(info, k) for k, _ in info._fields_}
 
+    def set_degree_order(self, stream=None) -> None:
+        """Renumber vertices internally by out-degree (inputs / outputs keep input ids)."""
+        check(lib().b2_graph_set_degree_order(self._h, C.c_void_p(_stream_ptr(stream))), "set_degree_order")
+
+    @property
+    def degree_ordered(self) -> bool:
+        return bool(lib().b2_graph_degree_ordered(self._h))
+
     def delta_heuristic(self, scale: float = 16.0) -> float:
         d = C.c_double()
         check(lib().b2_delta_heuristic(self._h, scale, C.byref(d)), "delta_heuristic")

@@ -91,6 +91,8 @@ _SIGS = {
     "b2_graph_create": (C.c_int, [C.POINTER(CSR), _P, C.POINTER(_P)]),
     "b2_graph_destroy": (C.c_int, [_P]),
     "b2_graph_info_get": (C.c_int, [_P, C.POINTER(GraphInfo)]),
+    "b2_graph_set_degree_order": (C.c_int, [_P, _P]),
+    "b2_graph_degree_ordered": (C.c_int32, [_P]),
     "b2_delta_heuristic": (C.c_int, [_P, C.c_double, C.POINTER(C.c_double)]),
     "b2_graph_trace": (C.c_int, [_P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     "b2_sssp_bf": (C.c_int, [_P, C.c_uint32, _P, _P, C.POINTER(Opts), _P, C.POINTER(Stats)]),

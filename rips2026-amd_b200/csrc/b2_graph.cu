@@ -194,6 +194,106 @@ b2_status finish_stats(b2_graph g, cudaStream_t st) {
   return B2_SUCCESS;
 }
 
+// ---- degree order ---------------------------------------------------------
+// On graphs with a few very high-degree vertices (RMAT, power-law) the
+// random label loads and dedup atomics of a solve hit L2 far more often when
+// the hot vertices sit next to each other: internal ids are assigned by
+// out-degree, descending (stable).  rowptr / edges are rebuilt in that order
+// with every destination renamed; solves and queries map the source id in
+// and scatter their outputs back through perm.
+__global__ void k_degrees(int64_t n, const uint64_t* rowptr, uint32_t* deg, uint32_t* ids) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    const uint64_t d = rowptr[v + 1] - rowptr[v];
+    deg[v] = (uint32_t)(d > 0xFFFFFFFFull ? 0xFFFFFFFFull : d);
+    ids[v] = (uint32_t)v;
+  }
+}
+__global__ void k_inverse(int64_t n, const uint32_t* perm, uint32_t* inv) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv[perm[i]] = (uint32_t)i;
+}
+// one warp per new row i: copy old row perm[i], renaming destinations
+__global__ void k_relabel_rows(int64_t n, const uint32_t* perm, const uint32_t* inv, const uint64_t* old_rp,
+                               const uint2* old_e, const uint64_t* new_rp, uint2* new_e) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (int64_t i = warp; i < n; i += nwarps) {
+    const uint64_t a = old_rp[perm[i]], len = old_rp[perm[i] + 1] - a, b = new_rp[i];
+    for (uint64_t k = lane; k < len; k += 32) {
+      const uint2 e = old_e[a + k];
+      new_e[b + k] = make_uint2(inv[e.x], e.y);
+    }
+  }
+}
+
+b2_status reorder_by_degree(b2_graph g, cudaStream_t st) {
+  if (g->perm || g->n < 2) return B2_SUCCESS;
+  const int64_t n = g->n, m = g->m;
+  DevBuf<uint32_t> deg, ids, sdeg;
+  DevBuf<unsigned char> tmp;
+  uint32_t *perm = nullptr, *inv = nullptr;
+  uint64_t* rp = nullptr;
+  uint2* ed = nullptr;
+  auto fail = [&](cudaError_t e) {
+    cudaFree(perm); cudaFree(inv); cudaFree(rp); cudaFree(ed);
+    return from_cuda(e);
+  };
+  cudaError_t e = deg.alloc((size_t)n);
+  if (e == cudaSuccess) e = ids.alloc((size_t)n);
+  if (e == cudaSuccess) e = sdeg.alloc((size_t)n + 1);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&perm, (size_t)n * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&inv, (size_t)n * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&rp, (size_t)(n + 1) * 8);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ed, std::max<size_t>((size_t)m, 1) * sizeof(uint2));
+  if (e != cudaSuccess) return fail(e);
+  k_degrees<<<grid_for(n, 256), 256, 0, st>>>(n, g->rowptr, deg.p, ids.p);
+  e = cudaGetLastError();
+  size_t tb = 0;
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, deg.p, sdeg.p, ids.p, perm, (int)n, 0, 32, st);
+  if (e == cudaSuccess) e = tmp.alloc(tb);
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, deg.p, sdeg.p, ids.p, perm, (int)n, 0, 32, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sdeg.p + n, 0, 4, st);
+  size_t tb2 = 0;
+  DevBuf<unsigned char> tmp2;
+  cub::TransformInputIterator<uint64_t, U32ToU64, const uint32_t*> it(sdeg.p, U32ToU64());
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, it, rp, n + 1, st);
+  if (e == cudaSuccess) e = tmp2.alloc(tb2);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp2.p, tb2, it, rp, n + 1, st);
+  if (e == cudaSuccess) {
+    k_inverse<<<grid_for(n, 256), 256, 0, st>>>(n, perm, inv);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && m) {
+    k_relabel_rows<<<grid_for(n * 32, 256), 256, 0, st>>>(n, perm, inv, g->rowptr, g->edges, rp, ed);
+    e = cudaGetLastError();
+  }
+  std::vector<uint32_t> hinv;
+  if (e == cudaSuccess) {
+    hinv.resize((size_t)n);
+    e = cudaMemcpyAsync(hinv.data(), inv, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(e);
+  cudaFree(g->rowptr);
+  cudaFree(g->edges);
+  g->rowptr = rp;
+  g->edges = ed;
+  g->perm = perm;
+  g->inv = inv;
+  g->inv_host.swap(hinv);
+  g->graph_bytes += (size_t)n * 8;
+  return B2_SUCCESS;
+}
+
+// Degree order pays off on large graphs whose degree distribution is skewed.
+bool wants_degree_order(b2_graph g) {
+  return g->n >= ((int64_t)1 << 23) && g->max_degree >= 64.0 * std::max(1.0, g->mean_degree);
+}
+
 // Order every adjacency list by weight (stable: equal weights keep their
 // order), so the edges with weight <= delta are a prefix of each row and a
 // light pass reads exactly them.  Stable segmented radix sort, keys = weight.
@@ -246,8 +346,9 @@ b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowpt
   cudaMemcpy(g->rowptr, rowptr, (size_t)(n + 1) * sizeof(uint64_t), cudaMemcpyDeviceToDevice);
   if (m) cudaMemcpy(g->edges, edges, (size_t)m * sizeof(uint2), cudaMemcpyDeviceToDevice);
   g->graph_bytes = (size_t)(n + 1) * 8 + (size_t)m * 8;
-  b2_status s = sort_rows_by_weight(g, 0);
-  if (s == B2_SUCCESS) s = finish_stats(g, 0);
+  b2_status s = finish_stats(g, 0);
+  if (s == B2_SUCCESS && wants_degree_order(g)) s = reorder_by_degree(g, 0);
+  if (s == B2_SUCCESS) s = sort_rows_by_weight(g, 0);
   if (s != B2_SUCCESS) { b2_graph_destroy(g); return s; }
   *out = g;
   return B2_SUCCESS;
@@ -398,8 +499,9 @@ extern "C" b2_status b2_graph_create(const b2_csr* csr, b2_stream stream, b2_gra
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   }
   if (e != cudaSuccess) { b2_graph_destroy(g); return from_cuda(e); }
-  b2_status s = sort_rows_by_weight(g, st);
-  if (s == B2_SUCCESS) s = finish_stats(g, st);
+  b2_status s = finish_stats(g, st);
+  if (s == B2_SUCCESS && wants_degree_order(g)) s = reorder_by_degree(g, st);
+  if (s == B2_SUCCESS) s = sort_rows_by_weight(g, st);
   if (s != B2_SUCCESS) { b2_graph_destroy(g); return s; }
   *out = g;
   return B2_SUCCESS;
@@ -409,7 +511,7 @@ extern "C" b2_status b2_graph_destroy(b2_graph g) {
   if (!g) return B2_INVALID_ARGUMENT;
   Workspace& w = g->ws;
   auto fr = [](void* p) { if (p) cudaFree(p); };
-  fr(g->rowptr); fr(g->edges); fr(g->in_rowptr32);
+  fr(g->rowptr); fr(g->edges); fr(g->in_rowptr32); fr(g->perm); fr(g->inv);
   fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
   fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
   fr(w.ctl); fr(w.reach);
@@ -417,6 +519,21 @@ extern "C" b2_status b2_graph_destroy(b2_graph g) {
   delete g;
   return B2_SUCCESS;
 }
+
+extern "C" b2_status b2_graph_set_degree_order(b2_graph g, b2_stream stream) {
+  if (!g) return B2_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g->mu);
+  const bool sorted = g->rows_sorted;
+  b2_status s = reorder_by_degree(g, (cudaStream_t)stream);
+  // relabelled rows keep each row's order, so weight-sorted rows stay sorted
+  g->rows_sorted = sorted;
+  g->ws.light_key_valid = 0;
+  g->features_valid = false;
+  g->pol_version = 0;
+  return s;
+}
+
+extern "C" int32_t b2_graph_degree_ordered(b2_graph g) { return (g && g->perm) ? 1 : 0; }
 
 extern "C" b2_status b2_graph_info_get(b2_graph g, b2_graph_info* info) {
   if (!g || !info) return B2_INVALID_ARGUMENT;

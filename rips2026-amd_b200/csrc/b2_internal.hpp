@@ -7,6 +7,7 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/b200sssp.h"
 
@@ -178,6 +179,11 @@ struct b2_graph_s {
   int32_t max_degree = 0;
   bool has_negative = false;
   bool rows_sorted = false;     // each adjacency list ordered by weight
+  // Degree order: internal vertex id i is the input vertex perm[i] (ids
+  // sorted by out-degree, descending); null when ids are the input's.
+  uint32_t* perm = nullptr;     // device, internal -> input id
+  uint32_t* inv = nullptr;      // device, input -> internal id
+  std::vector<uint32_t> inv_host;   // host copy of inv (source ids of solves and queries)
   size_t graph_bytes = 0;
   float features[24] = {};      // schedule-policy features (computed on first use)
   bool features_valid = false;
@@ -191,6 +197,8 @@ struct b2_graph_s {
 
 namespace b2 {
 b2_status ensure_workspace(b2_graph g, bool pred);
+// Internal id of input vertex `v` (identity unless the graph is in degree order).
+inline uint32_t internal_id(b2_graph g, uint32_t v) { return g->inv_host.empty() ? v : g->inv_host[v]; }
 // Learned schedule: delta multiplier (x Near-Far delta), fusion and light/heavy
 // choice for g.  B2_NOT_SUPPORTED when no policy is active.
 b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* lh_on);

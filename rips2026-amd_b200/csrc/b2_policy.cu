@@ -266,7 +266,9 @@ b2_status graph_features(b2_graph g, float* f) {
     b2_stats st;
     void* d = nullptr;
     B2_CUDA_TRY(cudaMalloc(&d, (size_t)g->n * 4));
-    b2_status s = b2_sssp_bf(g, src, d, nullptr, &o, 0, &st);
+    uint32_t src_in = src;   // sampled ids are internal; solves take input ids
+    if (g->perm) cudaMemcpy(&src_in, g->perm + src, 4, cudaMemcpyDeviceToHost);
+    b2_status s = b2_sssp_bf(g, src_in, d, nullptr, &o, 0, &st);
     cudaFree(d);
     if (s != B2_SUCCESS) return s;
     if (st.converged) depth = (double)st.iterations_used;

@@ -65,6 +65,7 @@ struct ServeQuery {
   uint32_t* out_dist;   // caller's buffer: device memory or mapped page-locked host memory
   int32_t* out_pred;    // nullable
   ServeRecord* rec;     // mapped page-locked host memory
+  const uint32_t* perm; // degree-ordered graph: internal -> input id (else null); source is internal
 };
 
 namespace {
@@ -351,9 +352,12 @@ __device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budg
     const uint32_t k = L::key(x);
     uint32_t out = k;
     if (W::kFloat) out = (k == kInfKey) ? 0x7f800000u : __float_as_uint(key_to_f32(k));
-    q.out_dist[v] = out;
-    if (PRED && q.out_pred)
-      q.out_pred[v] = (k == kInfKey || v == q.source) ? -1 : (int32_t)(uint32_t)(x & 0xFFFFFFFFull);
+    const uint32_t o = q.perm ? __ldg(q.perm + v) : v;   // input id of internal vertex v
+    q.out_dist[o] = out;
+    if (PRED && q.out_pred) {
+      const uint32_t pv = (uint32_t)(x & 0xFFFFFFFFull);
+      q.out_pred[o] = (k == kInfKey || v == q.source) ? -1 : (int32_t)(q.perm ? __ldg(q.perm + pv) : pv);
+    }
     if (k != kInfKey) {
       ++reached;
       redges += __ldg(q.rowptr + v + 1) - __ldg(q.rowptr + v);
@@ -563,7 +567,8 @@ b2_status srv_launch(b2_server s, Lane& ln) {
     d.rowptr = G.g->rowptr;
     d.edges = G.g->edges;
     d.n = G.n;
-    d.source = q.source;
+    d.source = internal_id(G.g, q.source);
+    d.perm = G.g->perm;
     d.is_float = G.isf ? 1u : 0u;
     d.pred = pred ? 1u : 0u;
     d.delta_u = G.delta_u;

@@ -94,6 +94,7 @@ struct Params {
   void* out_dist;
   int32_t* out_pred;
   uint32_t dist_is_out;   // `dist` aliases out_dist (no separate label buffer)
+  const uint32_t* perm;   // degree-ordered graph: internal -> input id of every output slot (else null)
   uint32_t is_float;
   uint32_t fusion;        // light frontiers up to this size run as a LOCAL phase (0: off)
   uint32_t adapt;         // ADDS: adjust the bucket width at window boundaries
@@ -1127,15 +1128,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
       for (size_t v = tid; v < P.n; v += stride) {
         const typename L::T wv = ldcg(srcl + v);
         const uint32_t k = L::key(wv);
+        const size_t o = P.perm ? (size_t)__ldg(P.perm + v) : v;   // input id of internal vertex v
         if (W::kFloat) {
-          ((float*)P.out_dist)[v] = (k == kInfKey) ? __uint_as_float(0x7f800000u) : key_to_f32(k);
+          ((float*)P.out_dist)[o] = (k == kInfKey) ? __uint_as_float(0x7f800000u) : key_to_f32(k);
         } else if (!P.dist_is_out || (const void*)srcl != P.out_dist) {
-          ((uint32_t*)P.out_dist)[v] = k;
+          ((uint32_t*)P.out_dist)[o] = k;
         }
         if (PRED && P.out_pred) {
           int32_t pr = -1;
-          if (k != kInfKey && v != P.source) pr = (int32_t)(uint32_t)(wv & 0xFFFFFFFFull);
-          P.out_pred[v] = pr;
+          if (k != kInfKey && v != P.source) {
+            const uint32_t pv = (uint32_t)(wv & 0xFFFFFFFFull);
+            pr = (int32_t)(P.perm ? __ldg(P.perm + pv) : pv);
+          }
+          P.out_pred[o] = pr;
         }
       }
     }
@@ -1278,7 +1283,8 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   Params P;
   memset(&P, 0, sizeof(P));
   P.n = (uint32_t)g->n;
-  P.source = source;
+  P.source = internal_id(g, source);
+  P.perm = g->perm;
   P.rowptr = g->rowptr;
   P.edges = g->edges;
   P.pstamp = w.pstamp;
@@ -1295,7 +1301,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   P.out_pred = d_pred;
   P.is_float = isf ? 1u : 0u;
   P.budget_ns = (unsigned long long)(std::max(1.0, o.timeout_ms > 0 ? o.timeout_ms : 20000.0) * 1.0e6);
-  if (pred) {
+  if (pred || g->perm) {   // labels in the workspace (degree order: outputs are scattered back)
     P.dist = w.dist_a;
     P.dist_cur = w.dist_b;
     P.dist_is_out = 0;
@@ -1432,7 +1438,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   if (stats && o.collect_reach) {
     unsigned long long* d_r = w.reach;   // workspace counters: no allocation (a cudaFree would sync the device)
     B2_CUDA_TRY(cudaMemsetAsync(d_r, 0, 16, st));
-    const void* lab = pred ? w.dist_a : d_dist;
+    const void* lab = (pred || g->perm) ? w.dist_a : d_dist;
     if (pred) k_reach<true><<<1024, 256, 0, st>>>(P.n, g->rowptr, lab, isf, d_r);
     else k_reach<false><<<1024, 256, 0, st>>>(P.n, g->rowptr, lab, isf, d_r);
     unsigned long long hr[2] = {0, 0};

@@ -26,6 +26,10 @@ def _dist_u32(t):
     return _np(t).view(np.uint32)
 
 
+def _raw(t, weight):
+    return _dist_u32(t) if weight == "u32" else _np(t)
+
+
 def _gpu_vs_dijkstra(b2, orc, hg, weight, sources, method="delta", pred=False, **opts):
     g = _graph(b2, hg, weight)
     w = hg.weights if weight == "u32" else hg.fweights
@@ -331,3 +335,52 @@ def test_adds_adaptive_width_exact(b2, orc, cuda, weight):
             if delta:
                 assert st["delta_updates"] > 0 and st["delta_final"] > delta
         g.close()
+
+
+@pytest.mark.parametrize("weight", ["u32", "f32"])
+def test_degree_order_keeps_input_ids(b2, orc, cuda, weight):
+    """A graph renumbered internally by degree answers in input ids: distances
+    bit-exact, predecessors a shortest-path tree, for every method, from the
+    server too, and the same words as the graph in input order."""
+    from b200sssp import serving
+    hg = b2.gen_rmat(13, 16, seed=21)
+    w = hg.weights if weight == "u32" else hg.fweights
+    plain = b2.Graph.from_host(hg, weight)
+    g = b2.Graph.from_host(hg, weight)
+    assert not g.degree_ordered
+    g.set_degree_order()
+    g.set_degree_order()                      # idempotent
+    assert g.degree_ordered
+    for s in (0, 77, hg.n - 1):
+        ref = orc.dijkstra(hg.rowptr, hg.colind, w, s)
+        for method in ("delta", "bf", "adds"):
+            d, p, st = g.sssp(s, method=method, pred=True)
+            got = _raw(d, weight)
+            assert np.array_equal(got, ref), method
+            assert orc.validate_spt(hg.rowptr, hg.colind, w, s, got, p.cpu().numpy()) == 0
+            d0, _, st0 = plain.sssp(s, method=method)
+            assert np.array_equal(got, _raw(d0, weight))
+            assert st["iterations_used"] == st0["iterations_used"]
+        d, _, st = g.sssp(s, collect_reach=1)
+        _, _, st0 = plain.sssp(s, collect_reach=1)
+        assert (st["reached"], st["reached_edges"]) == (st0["reached"], st0["reached_edges"])
+    srv = serving.Server(hbm_budget=64 << 20)
+    gid = srv.add_graph(g)
+    outs = []
+    for s in (5, 901):
+        out = srv.result_buffer(g)
+        pr = cuda.empty(g.n, dtype=cuda.int32).pin_memory()
+        srv.submit(gid, s, out, pr)
+        outs.append((s, out, pr))
+    srv.progress(wait_all=True)
+    assert all(c["status"] == 0 for c in srv.poll())
+    for s, out, pr in outs:
+        ref = orc.dijkstra(hg.rowptr, hg.colind, w, s)
+        got = out.numpy().view(np.uint32) if weight == "u32" else out.numpy()
+        assert np.array_equal(got, ref)
+        assert orc.validate_spt(hg.rowptr, hg.colind, w, s, got, pr.numpy()) == 0
+    srv.close()
+    f = __import__("b200sssp.policy", fromlist=["graph_features"]).graph_features(g)
+    assert np.isfinite(f).all()
+    g.close()
+    plain.close()
