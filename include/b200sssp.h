@@ -117,12 +117,16 @@ typedef struct b2_sssp_opts {
   int32_t check_interval;   /* for B2_BF_VAR_CHECKS */
   int32_t policy;           /* 0: fixed delta (opts.delta or the Near-Far heuristic);
                                1: learned (b2_policy_activate); overrides delta,
-                               light_heavy and a zero fusion_threshold */
+                               the push/pull switch and a zero fusion_threshold */
   double delta;             /* bucket width; <=0 selects the Near-Far heuristic */
   double delta_scale;       /* Near-Far constant C in delta = C * mean_w / mean_deg (16) */
   uint32_t hub_degree;      /* vertices with out-degree >= this are split into edge chunks */
   uint32_t fusion_threshold;/* frontier size under which one block runs sub-phases alone (0 = off) */
-  float pull_fraction;      /* reserved: frontier-edge fraction for pull mode (<=0 off) */
+  float pull_fraction;      /* push/pull switch of the delta-stepping heavy pass: pull (each
+                               unsettled vertex scans its heavy in-edges, weight order, early
+                               exit) when the bucket's members hold more than pull_fraction x n
+                               heavy out-edges (default 8); the incoming CSR is built on first
+                               use, only for graphs with m >= pull_fraction x n; <= 0: push only */
   uint32_t grid_blocks;     /* 0: occupancy-derived persistent grid */
   double timeout_ms;        /* bound on every device wait (default 20000) */
   int32_t collect_reach;    /* fill stats.reached / reached_edges (one extra O(n) pass) */
@@ -134,8 +138,8 @@ typedef struct b2_sssp_opts {
 } b2_sssp_opts;
 
 typedef struct b2_trace_entry {
-  uint32_t kind;        /* 1 relax, 2 commit, 3 far split, 4 probe, 5 output, 7 fused (one block);
-                           | 0x100 heavy pass */
+  uint32_t kind;        /* 1 relax, 2 commit, 3 far split, 4 probe, 5 output, 7 fused (one block),
+                           8 heavy pass by pull; | 0x100 heavy pass */
   uint32_t frontier;    /* frontier entries of the phase */
   uint32_t hub_chunks;  /* 256-edge chunks of split high-degree vertices */
   uint32_t bucket;      /* delta: bucket index; BF: round */
@@ -161,7 +165,7 @@ typedef struct b2_stats {
   uint32_t delta_updates;   /* ADDS: bucket-width changes */
   double delta_final;       /* ADDS: bucket width at the end (delta: = delta_used) */
   uint32_t policy_used;     /* 1: the learned policy chose delta / fusion / light-heavy */
-  uint32_t reserved1;
+  uint32_t heavy_pulls;     /* heavy passes run in the pull direction */
 } b2_stats;
 
 /* ---- library ---------------------------------------------------------- */
@@ -267,6 +271,10 @@ b2_status b2_policy_destroy(b2_policy p);
 /* params: 5955 floats; mu, sigma: 24 floats each (both NULL: unchanged). */
 b2_status b2_policy_set_params(b2_policy p, const float* params, const float* mu, const float* sigma);
 b2_status b2_policy_get_params(b2_policy p, float* params, float* mu, float* sigma);
+/* Solves keep the Near-Far delta when the network's |log2 multiplier| is below
+ * log2_dead_zone (chosen by cross-validation when the weights are trained;
+ * stored in the weight file).  Default 0. */
+b2_status b2_policy_set_dead_zone(b2_policy p, float log2_dead_zone);
 /* X: B x 24 raw features; Y: B x 3 outputs. */
 b2_status b2_policy_forward(b2_policy p, const float* X, int32_t B, float* Y);
 /* Gradient of the mean loss (y0-t0)^2 + BCE(y1,t1) + BCE(y2,t2) over the
@@ -299,8 +307,8 @@ b2_status b2_graph_features(b2_graph g, float* features);
 typedef struct b2_server_s* b2_server;
 typedef struct b2_server_opts {
   size_t hbm_budget_bytes;  /* device arena (default 1 GiB) */
-  int32_t max_batch;        /* queries per batch launch (default 1024) */
-  int32_t lanes;            /* streams with one batch in flight each (default 4) */
+  int32_t max_batch;        /* queries per batch launch (default 512) */
+  int32_t lanes;            /* streams with one batch in flight each (default 16) */
   int32_t max_inflight;     /* completion records (default 8192) */
   int32_t blocks_per_sm;    /* 0: occupancy limit */
   double timeout_ms;        /* per-query device budget (default 20000) */

@@ -236,7 +236,7 @@ class Graph:
         buf = (_lib.TraceEntry * cap)()
         n = C.c_int32()
         check(lib().b2_graph_trace(self._h, C.cast(buf, C.c_void_p), cap, C.byref(n)), "graph_trace")
-        kinds = {1: "relax", 2: "commit", 3: "split", 4: "probe", 5: "output", 7: "fused"}
+        kinds = {1: "relax", 2: "commit", 3: "split", 4: "probe", 5: "output", 7: "fused", 8: "pull"}
         out = []
         for e in buf[: n.value]:
             out.append({"kind": kinds.get(e.kind & 0xff, str(e.kind)) + ("-heavy" if e.kind & 0x100 else ""),

@@ -68,7 +68,7 @@ class Stats(C.Structure):
                 ("delta_used", C.c_double), ("kernel_ms", C.c_float), ("device_error", C.c_uint32),
                 ("grid_blocks", C.c_uint32), ("first_unchanged", C.c_uint32),
                 ("local_subphases", C.c_uint32), ("delta_updates", C.c_uint32),
-                ("delta_final", C.c_double), ("policy_used", C.c_uint32), ("reserved", C.c_uint32)]
+                ("delta_final", C.c_double), ("policy_used", C.c_uint32), ("heavy_pulls", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -114,6 +114,7 @@ _SIGS = {
     "b2_policy_destroy": (C.c_int, [_P]),
     "b2_policy_set_params": (C.c_int, [_P, _P, _P, _P]),
     "b2_policy_get_params": (C.c_int, [_P, _P, _P, _P]),
+    "b2_policy_set_dead_zone": (C.c_int, [_P, C.c_float]),
     "b2_policy_forward": (C.c_int, [_P, _P, C.c_int32, _P]),
     "b2_policy_gradient": (C.c_int, [_P, _P, _P, C.c_int32, _P, C.POINTER(C.c_float)]),
     "b2_policy_train": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float,

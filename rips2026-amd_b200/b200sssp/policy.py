@@ -1,4 +1,4 @@
-"""Learned schedule policy: graph features -> MLP -> (delta, fusion, light/heavy).
+"""Learned schedule policy: graph features -> MLP -> (delta, fusion, push/pull).
 
 No counterpart in the reference, which picks delta with the Near-Far rule
 (Charlotte_oneshot/sssp_hip.cpp:59-81, hip_adds_sssp.cpp:1080-1127); that rule
@@ -12,8 +12,9 @@ include/b200sssp.h).  This module adds:
 * weight files: ``.npz`` with ``format_version`` (``save_weights`` /
   ``load_weights``, pure numpy);
 * the label generator: a sweep of 16 log-spaced delta multipliers x fusion
-  on/off x light/heavy on/off with the delta-stepping kernel, timed on the
-  device, whose fastest configuration is the training target;
+  on/off x heavy pass push-only / push-or-pull (the default switch point)
+  with the delta-stepping kernel, timed on the device, whose fastest
+  configuration is the training target;
 * ``train_default``: builds a set of synthetic graphs (ER, RMAT, perturbed
   grids; uniform and lognormal weights), labels them, trains, and writes
   ``policy_weights.npz`` next to this file.
@@ -33,14 +34,15 @@ from ._lib import check, lib
 N_FEATURES = 24
 N_OUTPUTS = 3
 N_PARAMS = 5955
-FORMAT_VERSION = 1
+FORMAT_VERSION = 2   # 2: third output is the push/pull switch
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "policy_weights.npz")
 FEATURE_NAMES = [
     "log2_n", "log2_m", "avg_degree", "log2_1p_max_degree",
     "deg_q25", "deg_q50", "deg_q75", "deg_q90", "deg_q99", "zero_degree_frac",
     "w_q10", "w_q25", "w_q50", "w_q75", "w_q90", "log2_mean_w", "w_cv", "log2_1p_hop_depth",
     "log2_nearfar_delta", "light_frac", "is_float", "depth_capped", "w_q99", "log2_1p_avg_degree"]
-OUTPUT_NAMES = ["log2_delta_mult", "fusion_logit", "light_heavy_logit"]
+OUTPUT_NAMES = ["log2_delta_mult", "fusion_logit", "pull_logit"]
+PULL_ON = 8.0     # pull_fraction when the pull output is on (the library default)
 # delta multipliers of the label sweep: 2^(k/2), k = -5 .. 10 (16 log-spaced values)
 SWEEP_LOG2 = [k / 2.0 for k in range(-5, 11)]
 LOG2_MULT_RANGE = (-4.0, 6.0)     # the library clamps y0 to this range
@@ -90,7 +92,13 @@ class Policy:
         w = load_weights(path)
         p = cls(0)
         p.set_params(w["params"], w["mu"], w["sigma"])
+        p.set_dead_zone(float(w["dead_zone"]) if "dead_zone" in w else 0.0)
         return p
+
+    def set_dead_zone(self, log2_dead_zone: float) -> None:
+        """Keep the Near-Far delta when |predicted log2 multiplier| is below this."""
+        check(lib().b2_policy_set_dead_zone(self._h, C.c_float(log2_dead_zone)), "policy_set_dead_zone")
+        self.dead_zone = float(log2_dead_zone)
 
     def params(self):
         P = np.zeros(N_PARAMS, np.float32)
@@ -112,6 +120,7 @@ class Policy:
 
     def save(self, path: str, **meta) -> None:
         P, mu, sg = self.params()
+        meta.setdefault("dead_zone", np.float32(getattr(self, "dead_zone", 0.0)))
         save_weights(path, P, mu, sg, **meta)
 
     def forward(self, X) -> np.ndarray:
@@ -146,8 +155,11 @@ class Policy:
 
     def decide(self, features) -> dict:
         y = self.forward(np.asarray(features, np.float32).reshape(1, -1))[0]
-        return {"delta_mult": float(2.0 ** np.clip(y[0], *LOG2_MULT_RANGE)), "fusion": bool(y[1] > 0),
-                "light_heavy": bool(y[2] > 0)}
+        lm = float(np.clip(y[0], *LOG2_MULT_RANGE))
+        if abs(lm) < getattr(self, "dead_zone", 0.0):
+            lm = 0.0
+        return {"delta_mult": float(2.0 ** lm), "fusion": bool(y[1] > 0),
+                "pull": bool(y[2] > 0)}
 
     def close(self) -> None:
         if self._h:
@@ -181,7 +193,7 @@ def activate_default(path: str = DEFAULT_WEIGHTS) -> Policy:
 
 # ---- label generation ------------------------------------------------------
 def sweep(g, sources, method: str = "delta", reps: int = 1) -> dict:
-    """Time the schedule grid on g; returns {(log2_mult, fusion, lh): ms}.
+    """Time the schedule grid on g; returns {(log2_mult, fusion, pull): ms}.
 
     Device time of the persistent launches (stats.kernel_ms) summed over the
     sources; one untimed warm-up solve per configuration.  For integer weights
@@ -202,7 +214,7 @@ def sweep(g, sources, method: str = "delta", reps: int = 1) -> dict:
                 if key in seen:
                     out[(lm, fu, lh)] = seen[key]
                     continue
-                kw = dict(delta=delta, fusion_threshold=FUSION_ON if fu else 0, light_heavy=lh)
+                kw = dict(delta=delta, fusion_threshold=FUSION_ON if fu else 0, pull_fraction=PULL_ON if lh else 0.0)
                 g.sssp(int(sources[0]), method=method, out=dist, **kw)
                 ms = 0.0
                 for _ in range(reps):
@@ -215,7 +227,7 @@ def sweep(g, sources, method: str = "delta", reps: int = 1) -> dict:
 
 
 def label_from_sweep(times: dict, tol: float = 0.03):
-    """Target (log2 mult, fusion, lh) of the fastest configuration; among
+    """Target (log2 mult, fusion, pull) of the fastest configuration; among
     configurations within `tol` of the best the one nearest the Near-Far delta
     wins (labels stay stable under timing noise)."""
     best = min(times.values())
@@ -266,7 +278,7 @@ def training_graph(i: int, max_scale: int = 23, min_scale: int = 16):
 
 
 def times_array(times: dict) -> np.ndarray:
-    """Sweep dict -> [16 multipliers, fusion, light/heavy] array of ms."""
+    """Sweep dict -> [16 multipliers, fusion, pull] array of ms."""
     A = np.zeros((len(SWEEP_LOG2), 2, 2))
     for (lm, fu, lh), v in times.items():
         A[SWEEP_LOG2.index(lm), fu, lh] = v
@@ -337,17 +349,17 @@ def train_default(count: int = 200, max_scale: int = 23, epochs: int = 3000, lr:
 
 
 # ---- robust labels, decision cost, cross-validated training ---------------
-FIXED_INDEX = (SWEEP_LOG2.index(0.0), 0, 1)   # Near-Far delta, no fusion, light/heavy on
+FIXED_INDEX = (SWEEP_LOG2.index(0.0), 0, 1)   # Near-Far delta, no fusion, default push/pull switch
 
 
 def robust_label(A: np.ndarray, tol: float = 0.03) -> np.ndarray:
-    """Label of one sweep table A[16 multipliers, fusion, light/heavy] (ms).
+    """Label of one sweep table A[16 multipliers, fusion, pull] (ms).
 
     Each configuration is scored by its worst time over itself and its two
     neighbouring multipliers (x 2^-0.5, x 2^0.5) at the same fusion / split
     setting, so a label sits where the time is flat and a prediction that
     misses by half a step in log2 costs little.  Among scores within `tol` of
-    the best, the multiplier nearest 1 wins (then fusion off, split on)."""
+    the best, the multiplier nearest 1 wins (then fusion off, pull allowed)."""
     L = A.shape[0]
     score = np.empty_like(A)
     for i in range(L):
@@ -360,71 +372,87 @@ def robust_label(A: np.ndarray, tol: float = 0.03) -> np.ndarray:
     return np.array([SWEEP_LOG2[i], float(f), float(-nh)], np.float32)
 
 
-def decision_index(y) -> tuple[int, int, int]:
+def decision_index(y, dead_zone: float = 0.0) -> tuple[int, int, int]:
     """Sweep-grid configuration nearest to an MLP output (log2 mult, fusion
-    logit, light/heavy logit), with the library's clamp of the multiplier."""
+    logit, pull logit), with the library's clamp of the multiplier.  A
+    predicted |log2 multiplier| under `dead_zone` keeps the Near-Far delta
+    (the library applies the same rule, b2_policy_set_dead_zone)."""
     lm = float(np.clip(y[0], *LOG2_MULT_RANGE))
+    if abs(lm) < dead_zone:
+        lm = 0.0
     i = int(np.argmin([abs(lm - v) for v in SWEEP_LOG2]))
     return i, int(y[1] > 0), int(y[2] > 0)
 
 
-def decision_speedup(A: np.ndarray, y) -> float:
+def decision_speedup(A: np.ndarray, y, dead_zone: float = 0.0) -> float:
     """Fixed-schedule time over the time of the configuration y selects."""
-    return float(A[FIXED_INDEX] / A[decision_index(y)])
+    return float(A[FIXED_INDEX] / A[decision_index(y, dead_zone)])
+
+
+DEAD_ZONES = (0.0, 0.5, 0.75, 1.0, 1.5)
 
 
 def cross_validate(X, TT, folds: int = 5, seed: int = 0, epochs: int = 1500, lr: float = 3e-3,
                    weight_decay: float = 1e-2, tol: float = 0.03) -> dict:
     """k-fold estimate of the learned schedule's gain on unseen graphs: train
     on the other folds (GPU kernels), decide for each held-out graph, and read
-    the decision's time off its sweep table.  Returns the geometric-mean
-    speed-up over the fixed schedule, the fraction of graphs slower than
-    fixed, and the oracle (best-in-sweep) speed-up for reference."""
+    the decision's time off its sweep table.  Returns, per dead zone, the
+    geometric-mean speed-up over the fixed schedule, the fraction of graphs
+    slower than fixed and the worst case, plus the best-in-sweep speed-up."""
     X = np.asarray(X, np.float32)
     T = np.array([robust_label(a, tol) for a in TT], np.float32)
     idx = np.random.default_rng(seed).permutation(len(X))
-    sp = np.zeros(len(X))
+    Yall = np.zeros((len(X), N_OUTPUTS))
     for k in range(folds):
         test = idx[k::folds]
         train = np.setdiff1d(idx, test)
         p = Policy(seed=seed + k)
         p.train(X[train], T[train], epochs=epochs, lr=lr, weight_decay=weight_decay)
-        Y = p.forward(X[test])
-        for j, y in zip(test, Y):
-            sp[j] = decision_speedup(TT[j], y)
+        Yall[test] = p.forward(X[test])
         p.close()
     best = np.array([a[FIXED_INDEX] / a.min() for a in TT])
-    return {"geo_speedup": float(np.exp(np.log(sp).mean())), "slower_frac": float((sp < 0.99).mean()),
-            "worst": float(sp.min()), "oracle_geo_speedup": float(np.exp(np.log(best).mean())),
-            "per_graph": sp.tolist()}
+    out = {"oracle_geo_speedup": float(np.exp(np.log(best).mean())), "by_dead_zone": {}}
+    for dz in DEAD_ZONES:
+        sp = np.array([decision_speedup(a, y, dz) for a, y in zip(TT, Yall)])
+        out["by_dead_zone"][dz] = {"geo_speedup": float(np.exp(np.log(sp).mean())),
+                                   "slower_frac": float((sp < 0.99).mean()), "worst": float(sp.min()),
+                                   "per_graph": sp.tolist()}
+    return out
 
 
 def train_from_dataset(path: str, out: str | None = DEFAULT_WEIGHTS, grid=None, folds: int = 5, seed: int = 7,
                        log=print):
     """Relabel a saved sweep dataset with robust_label, pick (epochs, weight
-    decay, label tolerance) by cross-validated speed-up over the fixed
-    schedule, train on all graphs and save the weights with the
+    decay, label tolerance, dead zone) by cross-validated speed-up over the
+    fixed schedule, train on all graphs and save the weights with the
     cross-validation figures.  A larger tolerance keeps labels at the Near-Far
-    delta unless a configuration is clearly faster, which trades a little of
-    the gain for fewer graphs made slower than the fixed schedule."""
+    delta unless a configuration is clearly faster; a dead zone ignores
+    predicted changes of delta smaller than the network's typical error."""
     X, _, TT, info = load_dataset(path)
-    grid = grid or [(800, 1e-2, 0.03), (800, 1e-2, 0.08), (800, 1e-2, 0.15), (1500, 3e-2, 0.08),
-                    (1500, 3e-2, 0.15), (400, 1e-2, 0.08)]
+    grid = grid or [(800, 1e-2, 0.03), (800, 1e-2, 0.08), (1500, 3e-2, 0.08), (400, 1e-2, 0.08)]
     results = []
     for ep, wd, tol in grid:
         cv = cross_validate(X, TT, folds=folds, seed=seed, epochs=ep, weight_decay=wd, tol=tol)
-        log(f"cv epochs={ep} wd={wd} tol={tol}: geo speed-up {cv['geo_speedup']:.3f}, slower "
-            f"{cv['slower_frac']:.2f}, worst {cv['worst']:.3f} (best-in-sweep {cv['oracle_geo_speedup']:.3f})")
-        # rank by the geometric-mean gain, penalizing graphs made slower
-        results.append((cv["geo_speedup"] - 0.25 * cv["slower_frac"], ep, wd, tol, cv))
-    _, ep, wd, tol, cv = max(results, key=lambda r: r[0])
+        for dz, r in cv["by_dead_zone"].items():
+            log(f"cv epochs={ep} wd={wd} tol={tol} dead_zone={dz}: geo speed-up {r['geo_speedup']:.3f}, "
+                f"slower {r['slower_frac']:.2f}, worst {r['worst']:.3f} "
+                f"(best-in-sweep {cv['oracle_geo_speedup']:.3f})")
+            # rank by the geometric-mean gain, penalizing graphs made slower
+            results.append((r["geo_speedup"] - 0.25 * r["slower_frac"], ep, wd, tol, dz, r,
+                            cv["oracle_geo_speedup"]))
+    _, ep, wd, tol, dz, r, orc_sp = max(results, key=lambda t: t[0])
     T = np.array([robust_label(a, tol) for a in TT], np.float32)
-    p = train_on(X, T, epochs=ep, weight_decay=wd, seed=seed, out=out, label_tol=np.float32(tol),
-                 cv_geo_speedup=np.float32(cv["geo_speedup"]), cv_slower_frac=np.float32(cv["slower_frac"]),
-                 cv_worst=np.float32(cv["worst"]), cv_oracle_geo_speedup=np.float32(cv["oracle_geo_speedup"]),
-                 cv_folds=np.int32(folds))
-    log(f"trained on {len(X)} graphs (epochs={ep}, wd={wd}, tol={tol}) -> {out}")
-    return p, cv
+    p = train_on(X, T, epochs=ep, weight_decay=wd, seed=seed, out=None)
+    p.set_dead_zone(dz)
+    if out:
+        p.save(out, n_graphs=np.int32(len(X)), epochs=np.int32(ep), lr=np.float32(3e-3),
+               weight_decay=np.float32(wd), label_tol=np.float32(tol), dead_zone=np.float32(dz),
+               train_X=X, train_T=T, cv_geo_speedup=np.float32(r["geo_speedup"]),
+               cv_slower_frac=np.float32(r["slower_frac"]), cv_worst=np.float32(r["worst"]),
+               cv_oracle_geo_speedup=np.float32(orc_sp), cv_folds=np.int32(folds),
+               cv_per_graph=np.array(r["per_graph"], np.float32))
+    log(f"trained on {len(X)} graphs (epochs={ep}, wd={wd}, tol={tol}, dead_zone={dz}) -> {out}")
+    return p, r
 
 
 def compare(g, sources, method: str = "delta", reps: int = 3) -> dict:

@@ -64,7 +64,7 @@ def slot_bytes(n: int, with_pred: bool = False) -> int:
 
 
 class Server:
-    def __init__(self, hbm_budget: int = 1 << 30, max_batch: int = 1024, lanes: int = 4,
+    def __init__(self, hbm_budget: int = 1 << 30, max_batch: int = 512, lanes: int = 16,
                  max_inflight: int = 8192, timeout_ms: float = 20000.0, delta_scale: float = 4.0,
                  blocks_per_sm: int = 0):
         o = ServerOpts()

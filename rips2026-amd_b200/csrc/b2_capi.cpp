@@ -37,7 +37,7 @@ extern "C" void b2_sssp_opts_default(b2_sssp_opts* o) {
   o->delta_scale = 16.0;
   o->hub_degree = 256;
   o->fusion_threshold = 0;
-  o->pull_fraction = 0.0f;
+  o->pull_fraction = 8.0f;
   o->grid_blocks = 0;
   o->timeout_ms = 20000.0;
   o->collect_reach = 0;

@@ -297,9 +297,10 @@ bool wants_degree_order(b2_graph g) {
 // Order every adjacency list by weight (stable: equal weights keep their
 // order), so the edges with weight <= delta are a prefix of each row and a
 // light pass reads exactly them.  Stable segmented radix sort, keys = weight.
-b2_status sort_rows_by_weight(b2_graph g, cudaStream_t st) {
-  const int64_t m = g->m;
-  if (m < 2) return B2_SUCCESS;
+b2_status sort_segments_by_weight(int64_t n, int64_t m, const uint64_t* rowptr, uint2* edges, int weight_type,
+                                  cudaStream_t st, bool* sorted) {
+  *sorted = false;
+  if (m < 2) { *sorted = true; return B2_SUCCESS; }
   if (m > 0x7fffffffLL) return B2_SUCCESS;   // segmented sort item count is int; rows stay unsorted
   DevBuf<uint32_t> k0, k1, v0, v1;
   DevBuf<unsigned char> tmp;
@@ -307,28 +308,52 @@ b2_status sort_rows_by_weight(b2_graph g, cudaStream_t st) {
   B2_CUDA_TRY(k1.alloc((size_t)m));
   B2_CUDA_TRY(v0.alloc((size_t)m));
   B2_CUDA_TRY(v1.alloc((size_t)m));
-  k_unpack<<<grid_for(m, 256), 256, 0, st>>>(m, g->edges, k0.p, v0.p);
+  k_unpack<<<grid_for(m, 256), 256, 0, st>>>(m, edges, k0.p, v0.p);
   B2_CUDA_TRY(cudaGetLastError());
   size_t tb = 0;
-  const int nseg = (int)g->n;
-  if (g->weight_type == B2_W_F32) {
+  const int nseg = (int)n;
+  if (weight_type == B2_W_F32) {
     B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb, (const float*)k0.p, (float*)k1.p, v0.p, v1.p,
-                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+                                                          (int)m, nseg, rowptr, rowptr + 1, st));
     B2_CUDA_TRY(tmp.alloc(tb));
     B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(tmp.p, tb, (const float*)k0.p, (float*)k1.p, v0.p, v1.p,
-                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+                                                          (int)m, nseg, rowptr, rowptr + 1, st));
   } else {
     B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb, (const uint32_t*)k0.p, k1.p, v0.p, v1.p,
-                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+                                                          (int)m, nseg, rowptr, rowptr + 1, st));
     B2_CUDA_TRY(tmp.alloc(tb));
     B2_CUDA_TRY(cub::DeviceSegmentedSort::StableSortPairs(tmp.p, tb, (const uint32_t*)k0.p, k1.p, v0.p, v1.p,
-                                                          (int)m, nseg, g->rowptr, g->rowptr + 1, st));
+                                                          (int)m, nseg, rowptr, rowptr + 1, st));
   }
-  k_pack<<<grid_for(m, 256), 256, 0, st>>>(m, k1.p, v1.p, g->edges);
+  k_pack<<<grid_for(m, 256), 256, 0, st>>>(m, k1.p, v1.p, edges);
   B2_CUDA_TRY(cudaGetLastError());
   B2_CUDA_TRY(cudaStreamSynchronize(st));
-  g->rows_sorted = true;
+  *sorted = true;
   return B2_SUCCESS;
+}
+
+b2_status sort_rows_by_weight(b2_graph g, cudaStream_t st) {
+  bool sorted = false;
+  b2_status s = sort_segments_by_weight(g->n, g->m, g->rowptr, g->edges, g->weight_type, st, &sorted);
+  if (s == B2_SUCCESS) g->rows_sorted = sorted;
+  return s;
+}
+
+// ---- incoming CSR (pull direction) ----------------------------------------
+__global__ void k_in_degree(int64_t m, const uint2* e, uint32_t* deg) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) atomicAdd(&deg[e[i].x], 1u);
+}
+// one warp per outgoing row u: every edge u -> v lands in row v as (u, w)
+__global__ void k_in_fill(int64_t n, const uint64_t* rp, const uint2* e, unsigned long long* cursor, uint2* out) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (int64_t u = warp; u < n; u += nwarps)
+    for (uint64_t k = rp[u] + lane; k < rp[u + 1]; k += 32) {
+      const uint2 x = e[k];
+      out[atomicAdd(&cursor[x.x], 1ull)] = make_uint2((uint32_t)u, x.y);
+    }
 }
 
 }  // namespace
@@ -354,6 +379,52 @@ b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowpt
   return B2_SUCCESS;
 }
 
+// Incoming CSR in internal ids with weight-sorted rows; built once per graph
+// (the order of equal weights inside a row is not fixed, which no result
+// depends on: a pulled label is the minimum over the row).
+b2_status ensure_incoming(b2_graph g, cudaStream_t st) {
+  if (g->in_rowptr) return B2_SUCCESS;
+  const int64_t n = g->n, m = g->m;
+  DevBuf<uint32_t> deg;
+  DevBuf<unsigned long long> cursor;
+  DevBuf<unsigned char> tmp;
+  uint64_t* rp = nullptr;
+  uint2* ed = nullptr;
+  cudaError_t e = deg.alloc((size_t)n + 1);
+  if (e == cudaSuccess) e = cursor.alloc((size_t)n + 1);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&rp, (size_t)(n + 1) * 8);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ed, std::max<size_t>((size_t)m, 1) * sizeof(uint2));
+  if (e == cudaSuccess) e = cudaMemsetAsync(deg.p, 0, (size_t)(n + 1) * 4, st);
+  if (e == cudaSuccess && m) {
+    k_in_degree<<<grid_for(m, 256), 256, 0, st>>>(m, g->edges, deg.p);
+    e = cudaGetLastError();
+  }
+  size_t tb = 0;
+  cub::TransformInputIterator<uint64_t, U32ToU64, const uint32_t*> it(deg.p, U32ToU64());
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb, it, rp, n + 1, st);
+  if (e == cudaSuccess) e = tmp.alloc(tb);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp.p, tb, it, rp, n + 1, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cursor.p, rp, (size_t)(n + 1) * 8, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess && m) {
+    k_in_fill<<<grid_for(n * 32, 256), 256, 0, st>>>(n, g->rowptr, g->edges, cursor.p, ed);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  b2_status s = from_cuda(e);
+  bool sorted = false;
+  if (s == B2_SUCCESS) s = sort_segments_by_weight(n, m, rp, ed, g->weight_type, st, &sorted);
+  if (s == B2_SUCCESS && !sorted && m >= 2) s = B2_NOT_SUPPORTED;   // pull needs weight-sorted rows
+  if (s != B2_SUCCESS) {
+    cudaFree(rp);
+    cudaFree(ed);
+    return s;
+  }
+  g->in_rowptr = rp;
+  g->in_edges = ed;
+  g->graph_bytes += (size_t)(n + 1) * 8 + (size_t)m * 8;
+  return B2_SUCCESS;
+}
+
 b2_status ensure_workspace(b2_graph g, bool pred) {
   Workspace& w = g->ws;
   const size_t n = (size_t)g->n;
@@ -361,7 +432,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   // (Re)allocate.
   auto fr = [](void* p) { if (p) cudaFree(p); };
   fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
-  fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
+  fr(w.hstamp); fr(w.lightcnt); fr(w.in_lightcnt); fr(w.trace);
   fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   w = Workspace();
@@ -384,6 +455,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   if (e == cudaSuccess) e = al((void**)&w.farflag, n * 4);
   if (e == cudaSuccess) e = al((void**)&w.hstamp, n * 4);
   if (e == cudaSuccess) e = al((void**)&w.lightcnt, n * 4);
+  if (e == cudaSuccess) e = al((void**)&w.in_lightcnt, n * 4);
   if (e == cudaSuccess) e = al((void**)&w.trace, kTraceCap * sizeof(TraceEntry));
   if (e == cudaSuccess) e = al((void**)&w.queues, (5 + (size_t)kRing) * n * 4);
   if (e == cudaSuccess) e = al((void**)&w.hubs, 2 * w.hub_cap * sizeof(HubEntry));
@@ -392,7 +464,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   if (e == cudaSuccess) e = cudaMallocHost((void**)&w.h_ctl, sizeof(Control));
   if (e != cudaSuccess) {
     fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
-    fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
+    fr(w.hstamp); fr(w.lightcnt); fr(w.in_lightcnt); fr(w.trace);
     fr(w.ctl); fr(w.reach);
     if (w.h_ctl) cudaFreeHost(w.h_ctl);
     w = Workspace();
@@ -511,9 +583,9 @@ extern "C" b2_status b2_graph_destroy(b2_graph g) {
   if (!g) return B2_INVALID_ARGUMENT;
   Workspace& w = g->ws;
   auto fr = [](void* p) { if (p) cudaFree(p); };
-  fr(g->rowptr); fr(g->edges); fr(g->in_rowptr32); fr(g->perm); fr(g->inv);
+  fr(g->rowptr); fr(g->edges); fr(g->in_rowptr32); fr(g->perm); fr(g->inv); fr(g->in_rowptr); fr(g->in_edges);
   fr(w.dist_a); fr(w.dist_b); fr(w.pstamp); fr(w.bstamp); fr(w.farflag); fr(w.queues); fr(w.hubs);
-  fr(w.hstamp); fr(w.lightcnt); fr(w.trace);
+  fr(w.hstamp); fr(w.lightcnt); fr(w.in_lightcnt); fr(w.trace);
   fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   delete g;
@@ -528,6 +600,14 @@ extern "C" b2_status b2_graph_set_degree_order(b2_graph g, b2_stream stream) {
   // relabelled rows keep each row's order, so weight-sorted rows stay sorted
   g->rows_sorted = sorted;
   g->ws.light_key_valid = 0;
+  if (s == B2_SUCCESS && g->in_rowptr) {   // the incoming CSR was built in the old ids
+    cudaFree(g->in_rowptr);
+    cudaFree(g->in_edges);
+    g->graph_bytes -= (size_t)(g->n + 1) * 8 + (size_t)g->m * 8;
+    g->in_rowptr = nullptr;
+    g->in_edges = nullptr;
+  }
+  g->ws.in_light_key_valid = 0;
   g->features_valid = false;
   g->pol_version = 0;
   return s;

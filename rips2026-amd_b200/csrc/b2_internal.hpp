@@ -85,6 +85,7 @@ enum PhaseKind : uint32_t {
   kPhaseFinal = 5,     // write outputs
   kPhaseDone = 6,
   kPhaseLocal = 7,     // delta: block 0 alone runs small light sub-phases (bucket fusion)
+  kPhasePull = 8,      // delta: heavy pass in the pull direction (unsettled vertices scan in-edges)
 };
 
 enum QueueId : uint32_t {
@@ -124,6 +125,9 @@ struct Control {
   uint32_t far_min_key;    // adaptive mode: min distance key that landed in the far pile
   uint32_t far_min_key_next;
   unsigned long long win_frontier_sum;   // adaptive mode: frontier entries in this window
+  unsigned long long member_heavy;       // heavy out-edges of the current bucket's members (push cost)
+  uint32_t cur_min_key;                  // smallest label processed in the current bucket (pull bound)
+  uint32_t heavy_pulls;                  // heavy passes run by pull
   uint32_t win_phases;
   uint32_t delta_updates;
   // results
@@ -152,6 +156,9 @@ struct Workspace {
   uint32_t* lightcnt = nullptr; // per vertex: edges with weight <= delta (sorted prefix)
   uint32_t light_key_valid = 0;
   uint32_t light_key = 0;     // delta (uint32) or its float bits the counts were built for
+  uint32_t* in_lightcnt = nullptr;  // the same for the incoming rows (pull heavy pass)
+  uint32_t in_light_key_valid = 0;
+  uint32_t in_light_key = 0;
   TraceEntry* trace = nullptr;
   uint32_t trace_n = 0;       // entries recorded by the last traced solve
   uint32_t* queues = nullptr; // (5 + kRing) * n ids
@@ -173,7 +180,9 @@ struct b2_graph_s {
   int device = 0;
   uint64_t* rowptr = nullptr;   // outgoing, n + 1
   uint2* edges = nullptr;       // (dst, weight bits), m
-  uint32_t* in_rowptr32 = nullptr;  // reserved (pull mode)
+  uint32_t* in_rowptr32 = nullptr;  // reserved
+  uint64_t* in_rowptr = nullptr;    // incoming CSR (internal ids), rows sorted by weight; built on
+  uint2* in_edges = nullptr;        // first use by a solve that may pull its heavy pass
   double mean_weight = 1.0;     // over weights > 0
   double mean_degree = 0.0;
   int32_t max_degree = 0;
@@ -190,18 +199,19 @@ struct b2_graph_s {
   uint64_t pol_version = 0;     // policy decision cache: valid when equal to the
   double pol_mult = 1.0;        // active policy's version
   int32_t pol_fusion = 0;
-  int32_t pol_lh = 1;
+  int32_t pol_pull = 1;
   b2::Workspace ws;
   std::mutex mu;   // one solve at a time per handle
 };
 
 namespace b2 {
 b2_status ensure_workspace(b2_graph g, bool pred);
+b2_status ensure_incoming(b2_graph g, cudaStream_t st);
 // Internal id of input vertex `v` (identity unless the graph is in degree order).
 inline uint32_t internal_id(b2_graph g, uint32_t v) { return g->inv_host.empty() ? v : g->inv_host[v]; }
-// Learned schedule: delta multiplier (x Near-Far delta), fusion and light/heavy
+// Learned schedule: delta multiplier (x Near-Far delta), fusion and push/pull
 // choice for g.  B2_NOT_SUPPORTED when no policy is active.
-b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* lh_on);
+b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* pull_on);
 b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowptr, const uint2* edges,
                                      int weight_type, b2_graph* out);
 }  // namespace b2

@@ -1,5 +1,5 @@
 // Learned schedule policy: graph features -> MLP 24 -> 64 -> 64 -> 3 -> (delta
-// multiplier, bucket fusion on/off, light/heavy split on/off).
+// multiplier, bucket fusion on/off, push/pull switch of the heavy pass).
 //
 // No reference counterpart (the reference picks delta with the Near-Far rule,
 // Charlotte_oneshot/sssp_hip.cpp:59-81, and adapts it in hip_adds).  The
@@ -178,6 +178,7 @@ struct PolicyState {
   float* grad = nullptr;
   float mu[kIn];
   float sigma[kIn];
+  float dead_zone = 0.0f;   // |predicted log2 delta multiplier| below this keeps the Near-Far delta
   int step = 0;
 };
 
@@ -307,7 +308,7 @@ b2_status run_forward(b2_policy p, const float* xn_host, int B, float* y_host) {
 }
 }  // namespace
 
-b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* lh_on) {
+b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* pull_on) {
   std::lock_guard<std::mutex> lock(g_pol_mu);
   if (!g_active) return B2_NOT_SUPPORTED;
   if (g->pol_version != g_generation) {
@@ -317,14 +318,16 @@ b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int3
     normalize(g_active, g->features, xn, 1);
     s = run_forward(g_active, xn, 1, y);
     if (s != B2_SUCCESS) return s;
-    g->pol_mult = std::exp2(std::max(kLog2MultMin, std::min(kLog2MultMax, (double)y[0])));
+    double lm = std::max(kLog2MultMin, std::min(kLog2MultMax, (double)y[0]));
+    if (std::fabs(lm) < (double)g_active->s.dead_zone) lm = 0.0;
+    g->pol_mult = std::exp2(lm);
     g->pol_fusion = y[1] > 0.0f ? 1 : 0;
-    g->pol_lh = y[2] > 0.0f ? 1 : 0;
+    g->pol_pull = y[2] > 0.0f ? 1 : 0;
     g->pol_version = g_generation;
   }
   *delta_mult = g->pol_mult;
   *fusion_on = g->pol_fusion;
-  *lh_on = g->pol_lh;
+  *pull_on = g->pol_pull;
   return B2_SUCCESS;
 }
 
@@ -402,6 +405,14 @@ extern "C" b2_status b2_policy_set_params(b2_policy p, const float* params, cons
   std::lock_guard<std::mutex> lock(g_pol_mu);
   ++g_generation;
   return upload_params(p, params);
+}
+
+extern "C" b2_status b2_policy_set_dead_zone(b2_policy p, float log2_dead_zone) {
+  if (!p || !(log2_dead_zone >= 0.0f)) return B2_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_pol_mu);
+  p->s.dead_zone = log2_dead_zone;
+  ++g_generation;
+  return B2_SUCCESS;
 }
 
 extern "C" b2_status b2_policy_get_params(b2_policy p, float* params, float* mu, float* sigma) {

@@ -666,8 +666,8 @@ extern "C" void b2_server_opts_default(b2_server_opts* o) {
   if (!o) return;
   memset(o, 0, sizeof(*o));
   o->hbm_budget_bytes = (size_t)1 << 30;
-  o->max_batch = 1024;
-  o->lanes = 4;
+  o->max_batch = 512;
+  o->lanes = 16;   // concurrent batch launches: a long query holds only its own lane
   o->max_inflight = 8192;
   o->timeout_ms = 20000.0;
   o->delta_scale = 4.0;   // narrower than the full-GPU default: a CTA's phases end with block barriers

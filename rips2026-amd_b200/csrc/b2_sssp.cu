@@ -95,6 +95,10 @@ struct Params {
   int32_t* out_pred;
   uint32_t dist_is_out;   // `dist` aliases out_dist (no separate label buffer)
   const uint32_t* perm;   // degree-ordered graph: internal -> input id of every output slot (else null)
+  const uint64_t* __restrict__ in_rowptr;   // incoming CSR for the pull heavy pass (null: push only)
+  const uint2* __restrict__ in_edges;       // (source, weight bits), rows sorted by weight
+  const uint32_t* __restrict__ in_lightcnt; // light prefix of each incoming row
+  float pull_factor;      // pull when the members' heavy out-edges exceed pull_factor x n
   uint32_t is_float;
   uint32_t fusion;        // light frontiers up to this size run as a LOCAL phase (0: off)
   uint32_t adapt;         // ADDS: adjust the bucket width at window boundaries
@@ -437,9 +441,10 @@ __device__ __forceinline__ uint32_t src_key(const Params& P, uint32_t v) {
 // Edge range of v relaxed by this phase: the light prefix, the heavy suffix,
 // or the whole row.
 __device__ __forceinline__ void phase_range(const Params& P, const PhaseRec& R, uint32_t v, uint64_t& lo,
-                                            uint64_t& hi, bool& has_heavy) {
+                                            uint64_t& hi, bool& has_heavy, uint64_t* row_end = nullptr) {
   const uint64_t b = __ldg(&P.rowptr[v]);
   const uint64_t e = __ldg(&P.rowptr[v + 1]);
+  if (row_end) *row_end = e;
   has_heavy = false;
   if (P.lightcnt) {
     const uint64_t l = b + __ldg(&P.lightcnt[v]);
@@ -496,20 +501,34 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
   const bool members = MODE == kModeDelta && P.lightcnt && !R.heavy;
   const uint32_t i = base + lane;
   uint32_t v = 0, du = kInfKey;
-  uint64_t lo = 0, hi = 0;
+  uint64_t lo = 0, hi = 0, row_end = 0;
   bool valid = false, has_heavy = false;
   if (i < cnt) {
     v = ldcg(F + i);
     du = src_key<W, PRED, MODE>(P, v);
     valid = du != kInfKey;
     if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
-    if (valid) phase_range(P, R, v, lo, hi, has_heavy);
+    if (valid) phase_range(P, R, v, lo, hi, has_heavy, &row_end);
   }
   if (MODE == kModeDelta) {
     if (__any_sync(0xffffffffu, valid) && lane == 0 && ldcg(&c->bucket_valid) == 0) c->bucket_valid = 1;
     if (members) {
       // settled in this light round: its heavy suffix is relaxed once by the heavy phase
       const bool want = valid && has_heavy && atomicExch(&P.hstamp[v], R.hround) != R.hround;
+      if (P.in_rowptr) {
+        // push cost of the heavy pass and the bucket's smallest label (the pull's early-exit bound)
+        unsigned long long hv = want ? (unsigned long long)(row_end - hi) : 0ull;
+        uint32_t mk = valid ? du : 0xFFFFFFFFu;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          hv += __shfl_xor_sync(0xffffffffu, hv, o);
+          mk = min(mk, __shfl_xor_sync(0xffffffffu, mk, o));
+        }
+        if (lane == 0) {
+          if (hv) atomicAdd(&c->member_heavy, hv);
+          if (mk != 0xFFFFFFFFu) atomicMin(&c->cur_min_key, mk);
+        }
+      }
       stage(t.q.memb, t.q.nm, want, v);
       if (t.q.nm > kMemBuf / 2) {
         publish(P, &c->members_count, kQMembers, t.q.memb, t.q.nm, 14);
@@ -617,6 +636,60 @@ __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
   flush_all<MODE>(P, R, t.q, true);
 }
 
+// Heavy pass in the pull direction (delta mode).  The push pass relaxes the
+// heavy out-edges (w > delta) of every member, i.e. of every vertex whose label
+// lies in the current bucket.  Here each unsettled vertex v scans its heavy
+// in-edges in weight order and keeps the smallest (distance, source) word over
+// in-neighbours in the current bucket -- the same minimum the push pass's
+// atomics reach.  A member's label is at least lb (the smallest label of the
+// bucket), so once lb + w cannot beat v's best the rest of the row cannot
+// either and the scan stops.  One lane per vertex; improvements are routed
+// like pushed ones.
+template <class W, bool PRED>
+__device__ void pull_phase(const Params& P, const PhaseRec& R, Tally& t) {
+  using L = Label<PRED>;
+  typename L::T* lab = (typename L::T*)P.dist;
+  const uint32_t lb = ldcg(&P.ctl->cur_min_key);
+  const uint32_t lane = lane_id();
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t base = gwarp * 32; base < P.n; base += nwarps * 32) {
+    const uint32_t v = base + lane;
+    bool improved = false;
+    uint32_t best_key = kInfKey;
+    if (v < P.n && lb != 0xFFFFFFFFu) {
+      const typename L::T cw = ld_keep(lab + v, t.keep);
+      const uint32_t ck = L::key(cw);
+      if (ck == kInfKey || bucket_of<W>(R, ck) > R.cur) {
+        uint64_t e = __ldg(&P.in_rowptr[v]) + __ldg(&P.in_lightcnt[v]);
+        const uint64_t e1 = __ldg(&P.in_rowptr[v + 1]);
+        typename L::T best = cw;
+        unsigned long long scanned = 0;
+        for (; e < e1; ++e) {
+          const uint2 ed = __ldg(&P.in_edges[e]);
+          const uint32_t bound = W::extend(lb, ed.y);   // no member reaches v for less via this or later edges
+          if (PRED ? bound > L::key(best) : bound >= L::key(best)) break;
+          ++scanned;
+          const uint32_t ku = L::key(ld_keep(lab + ed.x, t.keep));
+          if (ku == kInfKey || bucket_of<W>(R, ku) != R.cur) continue;
+          const typename L::T cand = L::make(W::extend(ku, ed.y), ed.x);
+          if (cand < best) best = cand;
+        }
+        t.edges += scanned;
+        if (best < cw) {
+          const typename L::T old = atom_min_keep(lab + v, best, t.keep);
+          best_key = L::key(best);
+          improved = best_key < L::key(old);
+          t.impr += improved ? 1 : 0;
+        }
+      }
+    }
+    route<W, kModeDelta>(P, R, improved, v, best_key, t);
+    flush_all<kModeDelta>(P, R, t.q, false);
+  }
+  flush_all<kModeDelta>(P, R, t.q, true);
+}
+
 // ---------------------------------------------------------------------------
 // Manager steps (one thread, every other block parked at the barrier).
 __device__ __forceinline__ uint32_t vld(const uint32_t* p) { return *(const volatile uint32_t*)p; }
@@ -674,6 +747,8 @@ __device__ void manager_init(const Params& P) {
   r.dbase_b = 0;
   c->far_min_key = 0xFFFFFFFFu;
   c->far_min_key_next = 0xFFFFFFFFu;
+  c->cur_min_key = 0xFFFFFFFFu;
+  c->member_heavy = 0;
   store_rec(c, r);
 }
 
@@ -858,15 +933,30 @@ __device__ void manager_delta(const Params& P) {
       }
       const uint32_t mc = vld(&c->members_count);
       if (mc > 0) {              // light rounds of this bucket are done: heavy pass
-        nx.kind = kPhaseProcess;
         nx.heavy = 1;
-        nx.fq = kQMembers;
-        nx.fcount = mc;
+        const unsigned long long mh = vld64(&c->member_heavy);
+        c->member_heavy = 0;     // a later heavy pass of this bucket counts only its own members
+        if (P.in_rowptr && (double)mh > (double)P.pull_factor * (double)P.n) {
+          // push would relax more heavy edges than a pull over every vertex costs
+          c->members_count = 0;
+          c->heavy_pulls = vld(&c->heavy_pulls) + 1;
+          nx.kind = kPhasePull;
+          nx.fq = kQNone;
+          nx.fcount = P.n;
+          nx.hub_in_chunks = 0;
+          nx.hub_in_count = 0;
+        } else {
+          nx.kind = kPhaseProcess;
+          nx.fq = kQMembers;
+          nx.fcount = mc;
+        }
         store_rec(c, nx);
         return;
       }
     }
     // bucket r.cur is settled
+    c->cur_min_key = 0xFFFFFFFFu;
+    c->member_heavy = 0;
     if (vld(&c->bucket_valid)) {
       c->iterations = vld(&c->iterations) + 1;
       c->bucket_valid = 0;
@@ -1055,6 +1145,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
       process_phase<W, PRED, MODE>(P, R, t);
     } else if (R.kind == kPhaseLocal) {
       if (MODE == kModeDelta && blockIdx.x == 0) local_phase<W, PRED, MODE>(P, R, t);
+    } else if (R.kind == kPhasePull) {
+      if (MODE == kModeDelta) pull_phase<W, PRED>(P, R, t);
     } else if (R.kind == kPhaseCommit) {
       const uint32_t* F = queue_ptr(P, R.fq);
       for (size_t i = tid; i < R.fcount; i += stride) {
@@ -1248,6 +1340,21 @@ b2_status ensure_light_counts(b2_graph g, bool isf, uint32_t delta_u, float delt
   return B2_SUCCESS;
 }
 
+// The same light prefix for the incoming rows (pull heavy pass).
+b2_status ensure_in_light_counts(b2_graph g, bool isf, uint32_t delta_u, float delta_f, cudaStream_t st) {
+  Workspace& w = g->ws;
+  uint32_t key;
+  memcpy(&key, &delta_f, 4);
+  if (!isf) key = delta_u;
+  if (w.in_light_key_valid && w.in_light_key == key) return B2_SUCCESS;
+  k_light_count<<<1184, 256, 0, st>>>((uint32_t)g->n, g->in_rowptr, g->in_edges, isf ? 1 : 0, delta_u, delta_f,
+                                      w.in_lightcnt);
+  B2_CUDA_TRY(cudaGetLastError());
+  w.in_light_key = key;
+  w.in_light_key_valid = 1;
+  return B2_SUCCESS;
+}
+
 b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t* d_pred,
                    const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats, bool adds = false) {
   if (!g || !d_dist) return B2_INVALID_ARGUMENT;
@@ -1262,14 +1369,16 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     // learned schedule (computes and caches the graph's features on first use,
     // which runs solves of its own: before this solve takes the handle lock)
     double mult = 1.0;
-    int32_t fuse = 0, lh = 1;
-    const b2_status ps = policy_decide(g, &mult, &fuse, &lh);
+    int32_t fuse = 0, pull = 1;
+    const b2_status ps = policy_decide(g, &mult, &fuse, &pull);
     if (ps == B2_SUCCESS) {
       double nf = 1.0;
       b2_delta_heuristic(g, o.delta_scale > 0 ? o.delta_scale : 16.0, &nf);
       o.delta = nf * mult;
       if (o.fusion_threshold == 0) o.fusion_threshold = fuse ? 1024u : 0u;
-      o.light_heavy = lh;
+      // push/pull switch of the heavy pass: the default switch point, or push only
+      o.light_heavy = 1;
+      o.pull_fraction = pull ? (o.pull_fraction > 0.0f ? o.pull_fraction : 8.0f) : 0.0f;
       policy_used = 1;
     } else if (ps != B2_NOT_SUPPORTED) {
       return ps;
@@ -1347,6 +1456,16 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
       s = ensure_light_counts(g, isf, P.delta_u, df, st);
       if (s != B2_SUCCESS) return s;
       P.lightcnt = w.lightcnt;
+      // push/pull switch of the heavy pass: only graphs dense enough for a pull to pay off
+      if (o.pull_fraction > 0.0f && (double)g->m >= (double)o.pull_fraction * (double)g->n) {
+        s = ensure_incoming(g, st);
+        if (s == B2_SUCCESS) s = ensure_in_light_counts(g, isf, P.delta_u, df, st);
+        if (s != B2_SUCCESS) return s;
+        P.in_rowptr = g->in_rowptr;
+        P.in_edges = g->in_edges;
+        P.in_lightcnt = w.in_lightcnt;
+        P.pull_factor = o.pull_fraction;
+      }
     }
   }
   if (stats) {
@@ -1427,6 +1546,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     stats->first_unchanged = hc.first_unchanged;
     stats->local_subphases = hc.local_total;
     stats->delta_updates = hc.delta_updates;
+    stats->heavy_pulls = hc.heavy_pulls;
     if (mode == kModeDelta) {
       float inv;
       memcpy(&inv, &hc.rec.dinv, 4);

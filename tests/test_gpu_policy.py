@@ -83,19 +83,20 @@ def test_policy_sets_schedule_and_keeps_distances(pol, b2, orc, cuda, weight):
     w = hg.weights if weight == "u32" else hg.fweights
     ref = orc.dijkstra(hg.rowptr, hg.colind, w, 3)
     p = pol.Policy()
-    _set_constant(p, [2.0, -1.0, 1.0])            # delta x4, fusion off, light/heavy on
+    _set_constant(p, [2.0, -1.0, 1.0])            # delta x4, fusion off, pull allowed
     p.activate()
     d, _, st = g.sssp(3, policy=1)
     assert st["policy_used"] == 1
     want = max(1.0, np.floor(nf * 4.0)) if weight == "u32" else nf * 4.0
     assert st["delta_used"] == pytest.approx(want, rel=1e-12)
     assert np.array_equal(_raw(d, weight), ref)
-    _set_constant(p, [-9.0, 1.0, -1.0])            # clamped to /16, fusion on, split off
+    _set_constant(p, [-9.0, 1.0, -1.0])            # clamped to /16, fusion on, push only
     d2, _, st2 = g.sssp(3, policy=1, trace=1)
     assert st2["policy_used"] == 1
     want = max(1.0, np.floor(nf / 16.0)) if weight == "u32" else nf / 16.0
     assert st2["delta_used"] == pytest.approx(want, rel=1e-12)
-    assert not any(t["kind"].endswith("-heavy") for t in g.trace())
+    assert st2["heavy_pulls"] == 0
+    assert not any(t["kind"].startswith("pull") for t in g.trace())
     assert np.array_equal(_raw(d2, weight), ref)
     pol.Policy.deactivate()                        # no active policy: Near-Far fallback
     d3, _, st3 = g.sssp(3, policy=1)
@@ -128,3 +129,23 @@ def test_shipped_policy_keeps_distances(pol, b2, orc, cuda):
             assert np.array_equal(got, ref)
             assert orc.validate_spt(hg.rowptr, hg.colind, w, s, got, pr.cpu().numpy()) == 0
     p.deactivate()
+
+
+def test_dead_zone_keeps_near_far_delta(pol, b2, cuda):
+    """A predicted change of delta inside the dead zone is ignored: the solve
+    uses the Near-Far delta; outside it the multiplier applies."""
+    hg = b2.gen_rmat(13, 8, seed=6)
+    g = b2.Graph.from_host(hg, "f32")
+    nf = g.delta_heuristic()
+    p = pol.Policy()
+    _set_constant(p, [0.4, -1.0, 1.0])
+    p.set_dead_zone(0.5)
+    p.activate()
+    _, _, st = g.sssp(0, policy=1)
+    assert st["policy_used"] == 1 and st["delta_used"] == pytest.approx(nf, rel=1e-12)
+    p.set_dead_zone(0.3)
+    _, _, st = g.sssp(0, policy=1)
+    assert st["delta_used"] == pytest.approx(nf * 2.0 ** 0.4, rel=1e-6)
+    assert p.decide(pol.graph_features(g))["delta_mult"] == pytest.approx(2.0 ** 0.4, rel=1e-6)
+    pol.Policy.deactivate()
+    g.close()

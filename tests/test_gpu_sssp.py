@@ -384,3 +384,54 @@ def test_degree_order_keeps_input_ids(b2, orc, cuda, weight):
     assert np.isfinite(f).all()
     g.close()
     plain.close()
+
+
+@pytest.mark.parametrize("weight", ["u32", "f32"])
+def test_pull_heavy_pass_matches_push(b2, orc, cuda, weight):
+    """The pull direction of the heavy pass (forced with a tiny switch point)
+    gives the push pass's words exactly: distances, predecessors (smallest id
+    among equal distances) and bucket counts, for delta, ADDS and a
+    degree-ordered graph."""
+    graphs = [b2.gen_rmat(13, 16, seed=31), b2.gen_er(3000, 24000, 1, 1000, seed=32),
+              b2.gen_grid(40, 50, 0.05, seed=33)]
+    for k, hg in enumerate(graphs):
+        w = hg.weights if weight == "u32" else hg.fweights
+        g = b2.Graph.from_host(hg, weight)
+        if k == 0:
+            g.set_degree_order()
+        for method in ("delta", "adds"):
+            for s in (0, hg.n // 3):
+                ref = orc.dijkstra(hg.rowptr, hg.colind, w, s)
+                dp, pp, sp = g.sssp(s, method=method, pred=True, pull_fraction=0.0)
+                dq, pq, sq = g.sssp(s, method=method, pred=True, pull_fraction=1e-9)
+                assert sp["heavy_pulls"] == 0 and sq["heavy_pulls"] > 0
+                assert np.array_equal(_raw(dq, weight), ref)
+                assert np.array_equal(_raw(dq, weight), _raw(dp, weight))
+                assert np.array_equal(pq.cpu().numpy(), pp.cpu().numpy())
+                assert sq["iterations_used"] == sp["iterations_used"]
+                d2, _, _ = g.sssp(s, method=method, pull_fraction=1e-9)      # no predecessors
+                assert np.array_equal(_raw(d2, weight), ref)
+        g.close()
+
+
+def test_pull_switch_point(b2, orc, cuda):
+    """A dense skewed graph solved from its biggest hub pulls the heavy pass of
+    its first bucket once the members' heavy edges pass the switch point, and
+    still matches the oracle; a sparse grid never builds the incoming CSR."""
+    hg = b2.gen_rmat(15, 32, seed=41)
+    g = b2.Graph.from_host(hg, "u32")
+    hub = int(np.argmax(np.diff(hg.rowptr)))
+    d, _, st = g.sssp(hub, pull_fraction=2.0)
+    assert st["heavy_pulls"] >= 1
+    assert np.array_equal(_raw(d, "u32"), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, hub))
+    _, _, st = g.sssp(hub, pull_fraction=1e6)       # switch point never reached: push only
+    assert st["heavy_pulls"] == 0
+    grid = b2.gen_grid(64, 64, 0.0, seed=42)
+    gg = b2.Graph.from_host(grid, "u32")
+    gg.sssp(0, pull_fraction=0.0)                                # workspace allocated, push only
+    before = gg.info()["device_bytes"]
+    _, _, st = gg.sssp(0)
+    assert st["heavy_pulls"] == 0
+    assert gg.info()["device_bytes"] == before                   # no incoming CSR for a sparse grid
+    g.close()
+    gg.close()
