@@ -138,14 +138,14 @@ def test_dead_zone_keeps_near_far_delta(pol, b2, cuda):
     g = b2.Graph.from_host(hg, "f32")
     nf = g.delta_heuristic()
     p = pol.Policy()
-    _set_constant(p, [0.4, -1.0, 1.0])
+    _set_constant(p, [0.375, -1.0, 1.0])            # (exact in bfloat16)
     p.set_dead_zone(0.5)
     p.activate()
     _, _, st = g.sssp(0, policy=1)
     assert st["policy_used"] == 1 and st["delta_used"] == pytest.approx(nf, rel=1e-12)
-    p.set_dead_zone(0.3)
+    p.set_dead_zone(0.25)
     _, _, st = g.sssp(0, policy=1)
-    assert st["delta_used"] == pytest.approx(nf * 2.0 ** 0.4, rel=1e-6)
-    assert p.decide(pol.graph_features(g))["delta_mult"] == pytest.approx(2.0 ** 0.4, rel=1e-6)
+    assert st["delta_used"] == pytest.approx(nf * 2.0 ** 0.375, rel=1e-6)
+    assert p.decide(pol.graph_features(g))["delta_mult"] == pytest.approx(2.0 ** 0.375, rel=1e-6)
     pol.Policy.deactivate()
     g.close()
