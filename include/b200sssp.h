@@ -315,7 +315,10 @@ typedef struct b2_server_opts {
   double delta_scale;       /* Near-Far constant for each graph's bucket width (default 4:
                                one block's phases end with block barriers, so narrower buckets
                                with fewer wasted relaxations pay off) */
-  int32_t reserved[4];
+  int32_t big_vertices;     /* graphs with at least this many vertices are solved by a cluster of
+                               8 blocks (distributed shared memory, cluster barriers) on a
+                               quarter of the lanes; 0: 2^19; < 0: never */
+  int32_t reserved[3];
 } b2_server_opts;
 typedef struct b2_completion {
   uint64_t ticket;

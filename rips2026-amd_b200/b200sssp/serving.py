@@ -27,7 +27,7 @@ from ._lib import check, lib
 class ServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch", C.c_int32), ("lanes", C.c_int32),
                 ("max_inflight", C.c_int32), ("blocks_per_sm", C.c_int32), ("timeout_ms", C.c_double),
-                ("delta_scale", C.c_double), ("reserved", C.c_int32 * 4)]
+                ("delta_scale", C.c_double), ("big_vertices", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class Completion(C.Structure):
@@ -66,7 +66,7 @@ def slot_bytes(n: int, with_pred: bool = False) -> int:
 class Server:
     def __init__(self, hbm_budget: int = 1 << 30, max_batch: int = 512, lanes: int = 16,
                  max_inflight: int = 8192, timeout_ms: float = 20000.0, delta_scale: float = 4.0,
-                 blocks_per_sm: int = 0):
+                 blocks_per_sm: int = 0, big_vertices: int = 0):
         o = ServerOpts()
         lib().b2_server_opts_default(C.byref(o))
         o.hbm_budget_bytes = hbm_budget
@@ -76,6 +76,7 @@ class Server:
         o.timeout_ms = timeout_ms
         o.delta_scale = delta_scale
         o.blocks_per_sm = blocks_per_sm
+        o.big_vertices = big_vertices
         h = C.c_void_p()
         check(lib().b2_server_create(C.byref(o), C.byref(h)), "server_create")
         self._h = h

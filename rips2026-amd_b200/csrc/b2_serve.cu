@@ -29,8 +29,12 @@
 #include <random>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "b2_common.cuh"
 #include "b2_internal.hpp"
+
+namespace cg = cooperative_groups;
 
 namespace b2 {
 
@@ -71,7 +75,6 @@ struct ServeQuery {
 namespace {
 
 constexpr int kServeThreads = 512;
-constexpr int kServeWarps = kServeThreads / 32;
 constexpr uint32_t kBlockHubDeg = 512;     // rows at least this long are relaxed by the whole block
 constexpr uint32_t kHubListCap = 128;
 
@@ -117,6 +120,26 @@ struct SShared {
   uint32_t nhub;
   uint32_t hubs[kHubListCap];
   unsigned long long red[3];
+};
+
+// The team that solves one query: one thread block, or a cluster of
+// kClusterCTAs blocks (co-scheduled by the hardware) that share the lead
+// block's SShared through distributed shared memory and meet at cluster
+// barriers.  Large graphs get a cluster, so a long query runs on several SMs.
+constexpr uint32_t kClusterCTAs = 8;
+struct TeamCTA {
+  __device__ static uint32_t tid() { return threadIdx.x; }
+  __device__ static uint32_t threads() { return kServeThreads; }
+  __device__ static void sync() { __syncthreads(); }
+  template <class T>
+  __device__ static T* lead(T* p) { return p; }
+};
+struct TeamCluster {
+  __device__ static uint32_t tid() { return cg::this_cluster().block_rank() * kServeThreads + threadIdx.x; }
+  __device__ static uint32_t threads() { return kClusterCTAs * kServeThreads; }
+  __device__ static void sync() { cg::this_cluster().sync(); }
+  template <class T>
+  __device__ static T* lead(T* p) { return cg::this_cluster().map_shared_rank(p, 0); }
 };
 
 // Relax kSU edges per lane (u's label key -> v): all edge loads are issued
@@ -165,14 +188,14 @@ __device__ __forceinline__ void relax_edges(const ServeQuery& q, SShared& sh, co
 // One near phase: warps take 32-vertex chunks of the frontier and walk the
 // chunk's edges lane-parallel; rows of kBlockHubDeg or more edges are
 // collected and relaxed afterwards by the whole block.
-template <class W, bool PRED>
+template <class W, bool PRED, class Team>
 __device__ void near_phase(const ServeQuery& q, SShared& sh, const uint32_t* qcur, uint32_t* qnext,
                            uint32_t next_stamp, unsigned long long& edges) {
   using L = SLabel<PRED>;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t lane = threadIdx.x & 31u, warp = Team::tid() >> 5;
   const uint32_t cnt = sh.ncount;
   typename L::T* lab = (typename L::T*)q.labels;
-  for (uint32_t base = warp * 32; base < cnt; base += kServeWarps * 32) {
+  for (uint32_t base = warp * 32; base < cnt; base += Team::threads()) {
     const uint32_t i = base + lane;
     uint32_t u = 0, ukey = kInfKey, deg = 0;
     uint64_t start = 0;
@@ -218,21 +241,21 @@ __device__ void near_phase(const ServeQuery& q, SShared& sh, const uint32_t* qcu
     }
     edges += deg;
   }
-  __syncthreads();
+  Team::sync();
   const uint32_t nh = min(sh.nhub, kHubListCap);
   for (uint32_t h = 0; h < nh; ++h) {
     const uint32_t u = sh.hubs[h];
     const uint32_t ukey = L::key(__ldcg(lab + u));
     const uint64_t start = __ldg(q.rowptr + u), end = __ldg(q.rowptr + u + 1);
     const uint64_t len = end - start;
-    // every thread of the block runs the same number of iterations (warp_append needs whole warps)
-    for (uint64_t k0 = 0; k0 < len; k0 += (uint64_t)kServeThreads * kSU) {
+    // every thread of the team runs the same number of iterations (warp_append needs whole warps)
+    for (uint64_t k0 = 0; k0 < len; k0 += (uint64_t)Team::threads() * kSU) {
       uint32_t okey[kSU], ou[kSU];
       uint2 ed[kSU];
       bool valid[kSU];
 #pragma unroll
       for (int j = 0; j < kSU; ++j) {
-        const uint64_t k = k0 + (uint64_t)j * kServeThreads + threadIdx.x;
+        const uint64_t k = k0 + (uint64_t)j * Team::threads() + Team::tid();
         valid[j] = k < len;
         okey[j] = ukey;
         ou[j] = u;
@@ -240,22 +263,22 @@ __device__ void near_phase(const ServeQuery& q, SShared& sh, const uint32_t* qcu
       }
       relax_edges<W, PRED>(q, sh, okey, ou, ed, valid, next_stamp, qnext);
     }
-    if (threadIdx.x == 0) edges += len;
+    if (Team::tid() == 0) edges += len;
   }
 }
 
-template <class W, bool PRED>
-__device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budget_ns) {
+template <class W, bool PRED, class Team>
+__device__ void team_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budget_ns) {
   using L = SLabel<PRED>;
   typename L::T* lab = (typename L::T*)q.labels;
   const uint32_t n = q.n;
-  for (uint32_t v = threadIdx.x; v < n; v += kServeThreads) {
+  for (uint32_t v = Team::tid(); v < n; v += Team::threads()) {
     lab[v] = L::inf();
     q.stamp[v] = 0u;
     q.farflag[v] = 0u;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  Team::sync();
+  if (Team::tid() == 0) {
     lab[q.source] = L::make(W::zero_key(), kNoPred);
     q.qa[0] = q.source;
     q.stamp[q.source] = 1u;
@@ -266,7 +289,7 @@ __device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budg
     sh.stop = 0;
     sh.nhub = 0;
   }
-  __syncthreads();
+  Team::sync();
   unsigned long long edges = 0;
   uint32_t phase = 1;
   uint32_t* qcur = q.qa;
@@ -275,45 +298,45 @@ __device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budg
   for (;;) {
     // light phases of the current bucket
     while (sh.ncount > 0) {
-      near_phase<W, PRED>(q, sh, qcur, qnext, phase + 1, edges);
-      __syncthreads();
+      near_phase<W, PRED, Team>(q, sh, qcur, qnext, phase + 1, edges);
+      Team::sync();
       ++phase;
       uint32_t* t = qcur;
       qcur = qnext;
       qnext = t;
-      if (threadIdx.x == 0) {
+      if (Team::tid() == 0) {
         sh.ncount = sh.next_count;
         sh.next_count = 0;
         sh.nhub = 0;
         if (globaltimer_ns() - t0 > budget_ns) sh.stop = kErrTimeout;
         if (phase >= 0xFFFFFFF0u) sh.stop = kErrQueueOverflow;   // stamp space exhausted
       }
-      __syncthreads();
+      Team::sync();
       if (sh.stop) break;
     }
     if (sh.stop) { status = sh.stop; break; }
     if (sh.fcount == 0) break;
     // far split, pass 1: smallest live bucket above the current one
-    if (threadIdx.x == 0) sh.minb = kSNone;
-    __syncthreads();
+    if (Team::tid() == 0) sh.minb = kSNone;
+    Team::sync();
     const uint32_t fc = sh.fcount, cur = sh.cur;
     uint32_t mb = kSNone;
-    for (uint32_t i = threadIdx.x; i < fc; i += kServeThreads) {
+    for (uint32_t i = Team::tid(); i < fc; i += Team::threads()) {
       const uint32_t b = sbucket<W>(q, L::key(__ldcg(lab + q.fa[i])));
       if (b > cur && b < mb) mb = b;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mb = min(mb, __shfl_xor_sync(0xffffffffu, mb, o));
     if ((threadIdx.x & 31u) == 0 && mb != kSNone) atomicMin(&sh.minb, mb);
-    __syncthreads();
+    Team::sync();
     const uint32_t nb = sh.minb;
     if (nb == kSNone) break;                          // every far entry is settled
-    if (threadIdx.x == 0) { sh.cur = nb; sh.fnext = 0; sh.next_count = 0; }
-    __syncthreads();
+    if (Team::tid() == 0) { sh.cur = nb; sh.fnext = 0; sh.next_count = 0; }
+    Team::sync();
     // pass 2: entries of bucket nb go to the near queue, later ones are kept
     const uint32_t st = phase + 1;
-    for (uint32_t i0 = 0; i0 < fc; i0 += kServeThreads) {
-      const uint32_t i = i0 + threadIdx.x;
+    for (uint32_t i0 = 0; i0 < fc; i0 += Team::threads()) {
+      const uint32_t i = i0 + Team::tid();
       bool to_near = false, keep = false;
       uint32_t v = 0;
       if (i < fc) {
@@ -333,21 +356,21 @@ __device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budg
       const uint32_t pk = warp_append(&sh.fnext, keep);
       if (keep) q.fb[pk] = v;
     }
-    __syncthreads();
+    Team::sync();
     ++phase;
     uint32_t* t = q.fa;
     q.fa = q.fb;
     q.fb = t;
-    if (threadIdx.x == 0) {
+    if (Team::tid() == 0) {
       sh.ncount = sh.next_count;
       sh.next_count = 0;
       sh.fcount = sh.fnext;
     }
-    __syncthreads();
+    Team::sync();
   }
   // output into the caller's buffers, then the completion record
   unsigned long long reached = 0, redges = 0;
-  for (uint32_t v = threadIdx.x; v < n; v += kServeThreads) {
+  for (uint32_t v = Team::tid(); v < n; v += Team::threads()) {
     const typename L::T x = __ldcg(lab + v);
     const uint32_t k = L::key(x);
     uint32_t out = k;
@@ -364,8 +387,8 @@ __device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budg
     }
   }
   __threadfence_system();
-  if (threadIdx.x < 3) sh.red[threadIdx.x] = 0;
-  __syncthreads();
+  if (Team::tid() < 3) sh.red[Team::tid()] = 0;
+  Team::sync();
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     edges += __shfl_xor_sync(0xffffffffu, edges, o);
@@ -377,8 +400,8 @@ __device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budg
     atomicAdd(&sh.red[1], reached);
     atomicAdd(&sh.red[2], redges);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  Team::sync();
+  if (Team::tid() == 0) {
     ServeRecord* r = q.rec;
     r->status = status;
     r->phases = phase;
@@ -390,29 +413,45 @@ __device__ void cta_solve(ServeQuery& q, SShared& sh, uint64_t t0, uint64_t budg
   }
 }
 
-// Blocks take queries from the batch in order (one atomic per query) until
+// Teams take queries from the batch in order (one atomic per query) until
 // the batch is exhausted.  Descriptors live in mapped page-locked host memory.
-__global__ void __launch_bounds__(kServeThreads, 2)
-    k_serve(const ServeQuery* qs, uint32_t nq, uint32_t* next, unsigned long long budget_ns) {
-  __shared__ SShared sh;
-  __shared__ uint32_t s_q;
+template <class Team>
+__device__ __forceinline__ void serve_loop(const ServeQuery* qs, uint32_t nq, uint32_t* next,
+                                           unsigned long long budget_ns, SShared* sh_mine, uint32_t* q_mine) {
+  SShared& sh = *Team::lead(sh_mine);
+  uint32_t* s_q = Team::lead(q_mine);
   for (;;) {
-    if (threadIdx.x == 0) s_q = atomicAdd(next, 1u);
-    __syncthreads();
-    const uint32_t qi = s_q;
-    __syncthreads();
+    if (Team::tid() == 0) *s_q = atomicAdd(next, 1u);
+    Team::sync();
+    const uint32_t qi = *s_q;
+    Team::sync();
     if (qi >= nq) break;
     ServeQuery q = qs[qi];
     const uint64_t t0 = globaltimer_ns();
     if (q.is_float) {
-      if (q.pred) cta_solve<WF32, true>(q, sh, t0, budget_ns);
-      else cta_solve<WF32, false>(q, sh, t0, budget_ns);
+      if (q.pred) team_solve<WF32, true, Team>(q, sh, t0, budget_ns);
+      else team_solve<WF32, false, Team>(q, sh, t0, budget_ns);
     } else {
-      if (q.pred) cta_solve<WU32, true>(q, sh, t0, budget_ns);
-      else cta_solve<WU32, false>(q, sh, t0, budget_ns);
+      if (q.pred) team_solve<WU32, true, Team>(q, sh, t0, budget_ns);
+      else team_solve<WU32, false, Team>(q, sh, t0, budget_ns);
     }
-    __syncthreads();
+    Team::sync();
   }
+}
+
+__global__ void __launch_bounds__(kServeThreads, 2)
+    k_serve(const ServeQuery* qs, uint32_t nq, uint32_t* next, unsigned long long budget_ns) {
+  __shared__ SShared sh;
+  __shared__ uint32_t s_q;
+  serve_loop<TeamCTA>(qs, nq, next, budget_ns, &sh, &s_q);
+}
+
+// One query per cluster of kClusterCTAs blocks (grid: a multiple of it).
+__global__ void __cluster_dims__(kClusterCTAs, 1, 1) __launch_bounds__(kServeThreads, 2)
+    k_serve_cluster(const ServeQuery* qs, uint32_t nq, uint32_t* next, unsigned long long budget_ns) {
+  __shared__ SShared sh;
+  __shared__ uint32_t s_q;
+  serve_loop<TeamCluster>(qs, nq, next, budget_ns, &sh, &s_q);
 }
 
 }  // namespace
@@ -487,6 +526,7 @@ struct SrvGraph {
   b2_graph g;
   uint32_t n;
   bool isf;
+  bool big;             // solved by a block cluster instead of one block
   uint32_t delta_u;
   float inv_delta;
 };
@@ -508,6 +548,7 @@ struct Lane {
   uint32_t* d_next = nullptr;
   ServeQuery* h_desc = nullptr;   // mapped page-locked, max_batch entries
   bool busy = false;
+  bool big = false;               // launches cluster batches (queries on big graphs)
 };
 
 bool mapped_or_device(const void* p) {
@@ -538,23 +579,32 @@ struct b2_server_s {
   std::vector<int32_t> free_recs;
   uint64_t next_ticket = 1;
   uint32_t grid_cap = 0;
+  uint32_t cluster_cap = 0;   // clusters resident at once
+  uint32_t big_n = 0;         // graphs with at least this many vertices are big
   std::mutex mu;
 };
 
 namespace b2 {
 namespace {
 
+// One batch of queries of the lane's kind (big-graph queries on cluster lanes,
+// the others on block lanes), FIFO within the kind.  With a single lane the
+// lane takes the kind of the oldest pending query.
 b2_status srv_launch(b2_server s, Lane& ln) {
   std::vector<SrvQuery> batch;
-  while (!s->pending.empty() && (int32_t)batch.size() < s->o.max_batch && !s->free_recs.empty()) {
-    SrvQuery& q = s->pending.front();
+  bool big = ln.big;
+  if (s->lanes.size() < 2 && !s->pending.empty()) big = s->graphs[s->pending.front().gid].big;
+  for (auto it = s->pending.begin();
+       it != s->pending.end() && (int32_t)batch.size() < s->o.max_batch && !s->free_recs.empty();) {
+    SrvQuery& q = *it;
     const SrvGraph& G = s->graphs[q.gid];
+    if (G.big != big) { ++it; continue; }
     q.bytes = slot_bytes(G.n, q.out_pred != nullptr);
     if (!s->alloc.alloc(q.bytes, &q.off)) break;   // HBM budget: wait for running queries to finish
     q.rec = s->free_recs.back();
     s->free_recs.pop_back();
     batch.push_back(q);
-    s->pending.pop_front();
+    it = s->pending.erase(it);
   }
   if (batch.empty()) return B2_SUCCESS;
   for (size_t i = 0; i < batch.size(); ++i) {
@@ -588,11 +638,12 @@ b2_status srv_launch(b2_server s, Lane& ln) {
   }
   std::atomic_thread_fence(std::memory_order_seq_cst);
   const uint32_t nq = (uint32_t)batch.size();
-  const uint32_t grid = std::min(nq, s->grid_cap);
+  const uint32_t grid = big ? std::min(nq, s->cluster_cap) * kClusterCTAs : std::min(nq, s->grid_cap);
   // per-query device budget in ns (at least 1 ns: a tiny budget must still time out)
   const unsigned long long budget = (unsigned long long)std::max(1.0, s->o.timeout_ms * 1.0e6);
   B2_CUDA_TRY(cudaMemsetAsync(ln.d_next, 0, 4, ln.st));
-  k_serve<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
+  if (big) k_serve_cluster<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
+  else k_serve<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
   B2_CUDA_TRY(cudaGetLastError());
   B2_CUDA_TRY(cudaEventRecord(ln.done, ln.st));
   ln.busy = true;
@@ -708,6 +759,28 @@ extern "C" b2_status b2_server_create(const b2_server_opts* opts, b2_server* out
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
   if (o.blocks_per_sm > 0) per = std::min(per, o.blocks_per_sm);
   s->grid_cap = (uint32_t)std::max(1, per * sms);
+  {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kClusterCTAs);
+    cfg.blockDim = dim3(kServeThreads);
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = kClusterCTAs;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, (void*)k_serve_cluster, &cfg) != cudaSuccess || clusters < 1) {
+      cudaGetLastError();
+      clusters = std::max(1, (int)(s->grid_cap / (2 * kClusterCTAs)));
+    }
+    s->cluster_cap = (uint32_t)clusters;
+  }
+  s->big_n = o.big_vertices > 0 ? (uint32_t)o.big_vertices : (o.big_vertices < 0 ? 0xFFFFFFFFu : (1u << 19));
+  // a quarter of the lanes (at least one) launch cluster batches
+  const int nbig = std::max(1, o.lanes / 4);
+  for (int i = 0; i < o.lanes; ++i) s->lanes[i].big = o.lanes >= 2 && i >= o.lanes - nbig;
   *out = s;
   return B2_SUCCESS;
 }
@@ -737,6 +810,7 @@ extern "C" b2_status b2_server_add_graph(b2_server s, b2_graph g, int32_t* graph
   G.g = g;
   G.n = (uint32_t)g->n;
   G.isf = g->weight_type == B2_W_F32;
+  G.big = G.n >= s->big_n;
   double delta = 1.0;
   b2_delta_heuristic(g, s->o.delta_scale > 0 ? s->o.delta_scale : 4.0, &delta);
   if (G.isf) {

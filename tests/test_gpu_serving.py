@@ -201,3 +201,42 @@ def test_load_generator_results(srvmod, graphs, cuda, mode):
         d, _, _ = g.sssp(int(rep["query_source"][i]), method="delta")
         assert srvmod.checksum_words(d.cpu().numpy()) == int(rep["checksums"][i])
     srv.close()
+
+
+@pytest.mark.parametrize("big_vertices", [1, 4000])
+def test_cluster_teams_match_oracle_and_solver(srvmod, graphs, orc, cuda, big_vertices):
+    """Queries on big graphs are solved by a cluster of blocks sharing the lead
+    block's state through distributed shared memory: distances equal the
+    oracle's, predecessors equal the full-GPU solver's, and a query's words do
+    not change when it runs among others (every graph a cluster, or a mix)."""
+    torch = cuda
+    srv = srvmod.Server(hbm_budget=512 << 20, big_vertices=big_vertices)
+    gids = [srv.add_graph(x[2]) for x in graphs]
+    jobs = []
+    for (name, hg, g, w), gid in zip(graphs, gids):
+        for s in (0, g.n // 2, g.n - 1):
+            out = srv.result_buffer(g)
+            pr = torch.empty(g.n, dtype=torch.int32).pin_memory()
+            jobs.append((srv.submit(gid, s, out, pr), hg, g, w, s, out, pr))
+    # a mix of plain queries around them
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        k = int(rng.integers(0, len(graphs)))
+        srv.submit(gids[k], int(rng.integers(0, graphs[k][2].n)), srv.result_buffer(graphs[k][2]))
+    srv.progress(wait_all=True)
+    done = {c["ticket"]: c for c in srv.poll()}
+    assert all(c["status"] == 0 for c in done.values())
+    for t, hg, g, w, s, out, pr in jobs:
+        ref = orc.dijkstra(hg.rowptr, hg.colind, _w(hg, w), s)
+        assert np.array_equal(_raw(out, w), ref)
+        _, p_full, _ = g.sssp(s, method="delta", pred=True)
+        assert np.array_equal(pr.numpy(), p_full.cpu().numpy())
+        reached = int(np.count_nonzero(ref != (0xFFFFFFFF if w == "u32" else np.inf)))
+        assert done[t]["reached"] == reached
+    rep = srv.run_load(200, rate_qps=0.0, seed=9, record=True)
+    assert rep["completed"] == 200 and rep["failed"] == 0
+    for i in range(0, 200, 17):
+        _, hg, g, w = graphs[int(rep["query_graph"][i])]
+        ref = orc.dijkstra(hg.rowptr, hg.colind, _w(hg, w), int(rep["query_source"][i]))
+        assert int(rep["checksums"][i]) == srvmod.checksum_words(ref)
+    srv.close()
