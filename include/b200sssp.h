@@ -318,7 +318,10 @@ typedef struct b2_server_opts {
   int32_t big_vertices;     /* graphs with at least this many vertices are solved by a cluster of
                                8 blocks (distributed shared memory, cluster barriers) on a
                                quarter of the lanes; 0: 2^19; < 0: never */
-  int32_t reserved[3];
+  int32_t autotune;         /* 1: b2_server_add_graph times batches that fill the GPU under each
+                               team (block / cluster) x Near-Far constant (2, 4, 8) and keeps the
+                               fastest for that graph (needs an idle server); 0: the defaults */
+  int32_t reserved[2];
 } b2_server_opts;
 typedef struct b2_completion {
   uint64_t ticket;
@@ -344,6 +347,11 @@ void b2_server_opts_default(b2_server_opts* opts);
 b2_status b2_server_create(const b2_server_opts* opts, b2_server* out);
 b2_status b2_server_destroy(b2_server s);
 b2_status b2_server_add_graph(b2_server s, b2_graph g, int32_t* graph_id);
+/* The configuration a graph's queries run with: cluster team (1) or one block
+ * (0), the Near-Far constant of its bucket width, and whether the autotuner
+ * picked them. */
+b2_status b2_server_graph_config(b2_server s, int32_t graph_id, int32_t* cluster_team, double* delta_scale,
+                                 int32_t* tuned);
 /* Arena bytes one query on an n-vertex graph holds while it runs. */
 size_t b2_server_slot_bytes(int64_t n, int32_t with_pred);
 b2_status b2_server_submit(b2_server s, int32_t graph_id, uint32_t source, void* out_dist,

@@ -125,6 +125,8 @@ _SIGS = {
     "b2_server_create": (C.c_int, [_P, C.POINTER(_P)]),
     "b2_server_destroy": (C.c_int, [_P]),
     "b2_server_add_graph": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
+    "b2_server_graph_config": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_int32)]),
     "b2_server_slot_bytes": (C.c_size_t, [C.c_int64, C.c_int32]),
     "b2_server_submit": (C.c_int, [_P, C.c_int32, C.c_uint32, _P, _P, C.POINTER(C.c_uint64)]),
     "b2_server_cancel": (C.c_int, [_P, C.c_uint64]),

@@ -27,7 +27,8 @@ from ._lib import check, lib
 class ServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch", C.c_int32), ("lanes", C.c_int32),
                 ("max_inflight", C.c_int32), ("blocks_per_sm", C.c_int32), ("timeout_ms", C.c_double),
-                ("delta_scale", C.c_double), ("big_vertices", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("delta_scale", C.c_double), ("big_vertices", C.c_int32), ("autotune", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class Completion(C.Structure):
@@ -66,7 +67,7 @@ def slot_bytes(n: int, with_pred: bool = False) -> int:
 class Server:
     def __init__(self, hbm_budget: int = 1 << 30, max_batch: int = 512, lanes: int = 16,
                  max_inflight: int = 8192, timeout_ms: float = 20000.0, delta_scale: float = 4.0,
-                 blocks_per_sm: int = 0, big_vertices: int = 0):
+                 blocks_per_sm: int = 0, big_vertices: int = 0, autotune: bool = False):
         o = ServerOpts()
         lib().b2_server_opts_default(C.byref(o))
         o.hbm_budget_bytes = hbm_budget
@@ -77,6 +78,7 @@ class Server:
         o.delta_scale = delta_scale
         o.blocks_per_sm = blocks_per_sm
         o.big_vertices = big_vertices
+        o.autotune = 1 if autotune else 0
         h = C.c_void_p()
         check(lib().b2_server_create(C.byref(o), C.byref(h)), "server_create")
         self._h = h
@@ -87,6 +89,14 @@ class Server:
         check(lib().b2_server_add_graph(self._h, g._h, C.byref(gid)), "server_add_graph")
         self._graphs.append(g)
         return gid.value
+
+    def graph_config(self, graph_id: int) -> dict:
+        """Team, bucket-width constant and autotuned flag of a graph's queries."""
+        team, tuned = C.c_int32(), C.c_int32()
+        scale = C.c_double()
+        check(lib().b2_server_graph_config(self._h, graph_id, C.byref(team), C.byref(scale), C.byref(tuned)),
+              "server_graph_config")
+        return {"cluster_team": bool(team.value), "delta_scale": scale.value, "tuned": bool(tuned.value)}
 
     @staticmethod
     def result_buffer(g, pinned: bool = True):

@@ -527,8 +527,10 @@ struct SrvGraph {
   uint32_t n;
   bool isf;
   bool big;             // solved by a block cluster instead of one block
+  double delta_scale;   // Near-Far constant of the bucket width
   uint32_t delta_u;
   float inv_delta;
+  bool tuned;           // big / delta_scale were picked by measurement
 };
 
 struct SrvQuery {
@@ -549,7 +551,55 @@ struct Lane {
   ServeQuery* h_desc = nullptr;   // mapped page-locked, max_batch entries
   bool busy = false;
   bool big = false;               // launches cluster batches (queries on big graphs)
+  // The launch sequence of a batch (reset the query counter, run the teams)
+  // as an instantiated CUDA graph per team kind; each batch updates the
+  // kernel node's grid and arguments and replays it.
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  cudaGraphNode_t knode[2] = {nullptr, nullptr};
+  bool graph_failed = false;      // graph API refused: launch directly
 };
+
+// Build (once per lane and kind) or update the batch graph and launch it.
+cudaError_t launch_batch_graph(Lane& ln, bool big, uint32_t grid, uint32_t nq, unsigned long long budget) {
+  const int k = big ? 1 : 0;
+  const ServeQuery* desc = ln.h_desc;
+  uint32_t* next = ln.d_next;
+  void* args[] = {(void*)&desc, (void*)&nq, (void*)&next, (void*)&budget};
+  cudaKernelNodeParams kp;
+  memset(&kp, 0, sizeof(kp));
+  kp.func = big ? (void*)k_serve_cluster : (void*)k_serve;
+  kp.gridDim = dim3(grid);
+  kp.blockDim = dim3(kServeThreads);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = args;
+  cudaError_t e = cudaSuccess;
+  if (!ln.gexec[k]) {
+    cudaGraph_t graph = nullptr;
+    e = cudaGraphCreate(&graph, 0);
+    cudaGraphNode_t mnode = nullptr;
+    if (e == cudaSuccess) {
+      cudaMemsetParams mp;
+      memset(&mp, 0, sizeof(mp));
+      mp.dst = ln.d_next;
+      mp.value = 0;
+      mp.elementSize = 4;
+      mp.width = 1;
+      mp.height = 1;
+      e = cudaGraphAddMemsetNode(&mnode, graph, nullptr, 0, &mp);
+    }
+    if (e == cudaSuccess) e = cudaGraphAddKernelNode(&ln.knode[k], graph, &mnode, 1, &kp);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ln.gexec[k], graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      ln.gexec[k] = nullptr;
+      return e;
+    }
+  } else {
+    e = cudaGraphExecKernelNodeSetParams(ln.gexec[k], ln.knode[k], &kp);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaGraphLaunch(ln.gexec[k], ln.st);
+}
 
 bool mapped_or_device(const void* p) {
   if (!p) return false;
@@ -641,10 +691,20 @@ b2_status srv_launch(b2_server s, Lane& ln) {
   const uint32_t grid = big ? std::min(nq, s->cluster_cap) * kClusterCTAs : std::min(nq, s->grid_cap);
   // per-query device budget in ns (at least 1 ns: a tiny budget must still time out)
   const unsigned long long budget = (unsigned long long)std::max(1.0, s->o.timeout_ms * 1.0e6);
-  B2_CUDA_TRY(cudaMemsetAsync(ln.d_next, 0, 4, ln.st));
-  if (big) k_serve_cluster<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
-  else k_serve<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
-  B2_CUDA_TRY(cudaGetLastError());
+  cudaError_t ge = cudaErrorNotSupported;
+  if (!ln.graph_failed) {
+    ge = launch_batch_graph(ln, big, grid, nq, budget);
+    if (ge != cudaSuccess) {
+      cudaGetLastError();
+      ln.graph_failed = true;   // the same two launches, issued directly from now on
+    }
+  }
+  if (ge != cudaSuccess) {
+    B2_CUDA_TRY(cudaMemsetAsync(ln.d_next, 0, 4, ln.st));
+    if (big) k_serve_cluster<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
+    else k_serve<<<grid, kServeThreads, 0, ln.st>>>(ln.h_desc, nq, ln.d_next, budget);
+    B2_CUDA_TRY(cudaGetLastError());
+  }
   B2_CUDA_TRY(cudaEventRecord(ln.done, ln.st));
   ln.busy = true;
   for (auto& q : batch) s->running.push_back(q);
@@ -694,6 +754,70 @@ b2_status srv_progress(b2_server s) {
     if (st != B2_SUCCESS) return st;
   }
   return B2_SUCCESS;
+}
+
+// Autotuner: for one graph, time batches of queries that fill the GPU under
+// each candidate (team: one block or an 8-block cluster; Near-Far constant 2,
+// 4 or 8) and keep the configuration with the highest throughput.  Every
+// tuning query writes the same device buffer (results are discarded; the
+// stores do not interact).  Runs only on an idle server.
+b2_status set_bucket_width(SrvGraph& G, double scale);
+b2_status srv_submit(b2_server s, int32_t graph_id, uint32_t source, void* out_dist, int32_t* out_pred,
+                     uint64_t t_submit, bool check_ptrs, uint64_t* ticket);
+b2_status srv_tune_graph(b2_server s, int32_t gid) {
+  SrvGraph& G0 = s->graphs[gid];
+  const size_t slot = slot_bytes(G0.n, false);
+  uint32_t* d_out = nullptr;
+  B2_CUDA_TRY(cudaMalloc((void**)&d_out, (size_t)G0.n * 4));
+  const double scales[3] = {2.0, 4.0, 8.0};
+  double best_qps = -1.0;
+  bool best_big = s->graphs[gid].big;
+  double best_scale = s->graphs[gid].delta_scale;
+  b2_status status = B2_SUCCESS;
+  for (int team = 0; team < 2 && status == B2_SUCCESS; ++team) {
+    const uint32_t fill = team ? s->cluster_cap : s->grid_cap;
+    const size_t free_b = s->alloc.cap() - s->alloc.used();
+    const uint32_t q = (uint32_t)std::min<size_t>(std::min<size_t>(fill, (size_t)s->o.max_batch), free_b / slot);
+    if (q == 0) continue;
+    for (double sc : scales) {
+      SrvGraph& G = s->graphs[gid];
+      G.big = team == 1;
+      if (set_bucket_width(G, sc) != B2_SUCCESS) continue;
+      double elapsed = 0.0;
+      uint64_t done_q = 0;
+      for (int rep = 0; rep < 8 && status == B2_SUCCESS; ++rep) {
+        const uint64_t t0 = now_ns();
+        for (uint32_t i = 0; i < q; ++i) {
+          uint64_t tk = 0;
+          status = srv_submit(s, gid, (uint32_t)(((uint64_t)i * 2654435761ull) % G.n), d_out, nullptr, t0, false,
+                              &tk);
+          if (status != B2_SUCCESS) break;
+        }
+        const uint64_t tlim = t0 + (uint64_t)(4.0 * s->o.timeout_ms * 1e6) + 60000000000ull;
+        while (status == B2_SUCCESS && (!s->pending.empty() || !s->running.empty())) {
+          status = srv_progress(s);
+          if (now_ns() > tlim) status = B2_TIMEOUT;
+        }
+        s->done.clear();
+        if (rep == 0) continue;                    // warm-up batch
+        elapsed += (double)(now_ns() - t0) * 1e-9;
+        done_q += q;
+        if (elapsed > 0.05 && rep >= 2) break;
+      }
+      const double qps = elapsed > 0 ? (double)done_q / elapsed : 0.0;
+      if (qps > best_qps) {
+        best_qps = qps;
+        best_big = team == 1;
+        best_scale = sc;
+      }
+    }
+  }
+  cudaFree(d_out);
+  SrvGraph& G = s->graphs[gid];
+  G.big = best_big;
+  b2_status st2 = set_bucket_width(G, best_scale);
+  G.tuned = status == B2_SUCCESS && st2 == B2_SUCCESS;
+  return status != B2_SUCCESS ? status : st2;
 }
 
 // Whole device: cancel nothing, wait for every running query (bounded by the
@@ -790,6 +914,8 @@ extern "C" b2_status b2_server_destroy(b2_server s) {
   for (auto& ln : s->lanes)
     if (ln.st) cudaStreamSynchronize(ln.st);
   for (auto& ln : s->lanes) {
+    for (int k = 0; k < 2; ++k)
+      if (ln.gexec[k]) cudaGraphExecDestroy(ln.gexec[k]);
     if (ln.st) cudaStreamDestroy(ln.st);
     if (ln.done) cudaEventDestroy(ln.done);
     cudaFree(ln.d_next);
@@ -801,6 +927,27 @@ extern "C" b2_status b2_server_destroy(b2_server s) {
   return B2_SUCCESS;
 }
 
+namespace b2 {
+namespace {
+b2_status set_bucket_width(SrvGraph& G, double scale) {
+  double delta = 1.0;
+  b2_delta_heuristic(G.g, scale, &delta);
+  if (G.isf) {
+    const float df = (float)delta;
+    if (!(df > 0.0f) || !std::isfinite(df)) return B2_INVALID_ARGUMENT;
+    G.inv_delta = 1.0f / df;
+    G.delta_u = 1;
+  } else {
+    G.delta_u = (uint32_t)std::min(4294967295.0, std::max(1.0, std::floor(delta)));
+    G.inv_delta = 0.0f;
+  }
+  G.delta_scale = scale;
+  return B2_SUCCESS;
+}
+b2_status srv_tune_graph(b2_server s, int32_t gid);
+}  // namespace
+}  // namespace b2
+
 extern "C" b2_status b2_server_add_graph(b2_server s, b2_graph g, int32_t* graph_id) {
   if (!s || !g || !graph_id) return B2_INVALID_ARGUMENT;
   if (g->has_negative) return B2_INVALID_WEIGHT;
@@ -811,19 +958,31 @@ extern "C" b2_status b2_server_add_graph(b2_server s, b2_graph g, int32_t* graph
   G.n = (uint32_t)g->n;
   G.isf = g->weight_type == B2_W_F32;
   G.big = G.n >= s->big_n;
-  double delta = 1.0;
-  b2_delta_heuristic(g, s->o.delta_scale > 0 ? s->o.delta_scale : 4.0, &delta);
-  if (G.isf) {
-    const float df = (float)delta;
-    if (!(df > 0.0f) || !std::isfinite(df)) return B2_INVALID_ARGUMENT;
-    G.inv_delta = 1.0f / df;
-    G.delta_u = 1;
-  } else {
-    G.delta_u = (uint32_t)std::min(4294967295.0, std::max(1.0, std::floor(delta)));
-    G.inv_delta = 0.0f;
-  }
+  G.tuned = false;
+  b2_status st = set_bucket_width(G, s->o.delta_scale > 0 ? s->o.delta_scale : 4.0);
+  if (st != B2_SUCCESS) return st;
   s->graphs.push_back(G);
   *graph_id = (int32_t)s->graphs.size() - 1;
+  if (s->o.autotune) {
+    if (!s->pending.empty() || !s->running.empty()) return B2_SUCCESS;   // busy: keep the defaults
+    st = srv_tune_graph(s, *graph_id);
+    if (st != B2_SUCCESS) {
+      s->graphs.pop_back();
+      return st;
+    }
+  }
+  return B2_SUCCESS;
+}
+
+extern "C" b2_status b2_server_graph_config(b2_server s, int32_t graph_id, int32_t* cluster_team,
+                                            double* delta_scale, int32_t* tuned) {
+  if (!s) return B2_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (graph_id < 0 || graph_id >= (int32_t)s->graphs.size()) return B2_INVALID_ARGUMENT;
+  const SrvGraph& G = s->graphs[graph_id];
+  if (cluster_team) *cluster_team = G.big ? 1 : 0;
+  if (delta_scale) *delta_scale = G.delta_scale;
+  if (tuned) *tuned = G.tuned ? 1 : 0;
   return B2_SUCCESS;
 }
 

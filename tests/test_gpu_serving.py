@@ -240,3 +240,24 @@ def test_cluster_teams_match_oracle_and_solver(srvmod, graphs, orc, cuda, big_ve
         ref = orc.dijkstra(hg.rowptr, hg.colind, _w(hg, w), int(rep["query_source"][i]))
         assert int(rep["checksums"][i]) == srvmod.checksum_words(ref)
     srv.close()
+
+
+def test_autotuned_server_matches_oracle(srvmod, graphs, orc):
+    """With autotune the server times each graph under every team kind and
+    bucket-width constant before admitting queries; answers stay exact."""
+    srv = srvmod.Server(hbm_budget=512 << 20, autotune=True)
+    gids = [srv.add_graph(x[2]) for x in graphs[:3]]
+    for gid in gids:
+        cfg = srv.graph_config(gid)
+        assert cfg["tuned"] and cfg["delta_scale"] in (2.0, 4.0, 8.0)
+    jobs = []
+    for (name, hg, g, w), gid in zip(graphs[:3], gids):
+        for s in (0, g.n // 3):
+            out = srv.result_buffer(g)
+            jobs.append((srv.submit(gid, s, out), hg, w, s, out))
+    srv.progress(wait_all=True)
+    done = {c["ticket"]: c for c in srv.poll()}
+    for t, hg, w, s, out in jobs:
+        assert done[t]["status"] == 0
+        assert np.array_equal(_raw(out, w), orc.dijkstra(hg.rowptr, hg.colind, _w(hg, w), s))
+    srv.close()
