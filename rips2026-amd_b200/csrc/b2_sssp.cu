@@ -298,18 +298,29 @@ __device__ __forceinline__ void publish_slots(const Params& P, WarpQ& q) {
     for (uint32_t i = lane_id(); i < q.ns; i += 32)
       if (q.slotb[2 * i + 1] == s0) dst[pos++] = q.slotb[2 * i];
     __syncwarp();
-    // compact the entries of other slots to the front (single lane keeps order simple)
-    uint32_t kept = 0;
-    if (lane_id() == 0) {
-      for (uint32_t i = 0; i < q.ns; ++i)
-        if (q.slotb[2 * i + 1] != s0) {
-          q.slotb[2 * kept] = q.slotb[2 * i];
-          q.slotb[2 * kept + 1] = q.slotb[2 * i + 1];
-          ++kept;
-        }
+    if (total == q.ns) {   // one slot only (the usual case)
+      q.ns = 0;
+      return;
     }
-    kept = __shfl_sync(0xffffffffu, kept, 0);
-    __syncwarp();
+    // compact the entries of other slots to the front, 32 at a time: every
+    // lane reads its entry before any lane writes, and a write position never
+    // passes the chunk being read
+    uint32_t kept = 0;
+    for (uint32_t i0 = 0; i0 < q.ns; i0 += 32) {
+      const uint32_t i = i0 + lane_id();
+      uint32_t ev = 0, es = s0;
+      if (i < q.ns) { ev = q.slotb[2 * i]; es = q.slotb[2 * i + 1]; }
+      const bool keep = es != s0;
+      const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+      __syncwarp();
+      if (keep) {
+        const uint32_t d = kept + __popc(bal & ((1u << lane_id()) - 1u));
+        q.slotb[2 * d] = ev;
+        q.slotb[2 * d + 1] = es;
+      }
+      kept += __popc(bal);
+      __syncwarp();
+    }
     q.ns = kept;
     remaining = kept;
   }
