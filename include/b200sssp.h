@@ -134,12 +134,19 @@ typedef struct b2_sssp_opts {
   int32_t light_heavy;      /* delta: relax light edges (w <= delta) per sub-phase and heavy
                                edges once per settled vertex (default 1) */
   int32_t trace;            /* record one b2_trace_entry per phase (b2_graph_trace) */
-  int32_t reserved[4];
+  float dense_fraction;     /* delta / ADDS: a near or window-slot frontier of at least
+                               dense_fraction x n vertices is found by sweeping the per-vertex
+                               push / bucket stamps in vertex order instead of reading its
+                               queue (ordered access to labels and rows); 0 (default): 1/16
+                               on graphs whose largest out-degree is <= 64, else the queue;
+                               < 0: always the queue */
+  int32_t reserved[3];
 } b2_sssp_opts;
 
 typedef struct b2_trace_entry {
   uint32_t kind;        /* 1 relax, 2 commit, 3 far split, 4 probe, 5 output, 7 fused (one block),
-                           8 heavy pass by pull; | 0x100 heavy pass */
+                           8 heavy pass by pull; | 0x100 heavy pass; | 0x200 frontier found by
+                           a stamp sweep */
   uint32_t frontier;    /* frontier entries of the phase */
   uint32_t hub_chunks;  /* 256-edge chunks of split high-degree vertices */
   uint32_t bucket;      /* delta: bucket index; BF: round */

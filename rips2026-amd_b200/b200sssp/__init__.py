@@ -239,7 +239,8 @@ class Graph:
         kinds = {1: "relax", 2: "commit", 3: "split", 4: "probe", 5: "output", 7: "fused", 8: "pull"}
         out = []
         for e in buf[: n.value]:
-            out.append({"kind": kinds.get(e.kind & 0xff, str(e.kind)) + ("-heavy" if e.kind & 0x100 else ""),
+            out.append({"kind": kinds.get(e.kind & 0xff, str(e.kind)) + ("-heavy" if e.kind & 0x100 else "")
+                        + ("-dense" if e.kind & 0x200 else ""),
                         "frontier": e.frontier, "hub_chunks": e.hub_chunks, "bucket": e.bucket,
                         "t_us": e.t_ns / 1e3})
         return out

@@ -52,7 +52,7 @@ class Opts(C.Structure):
                 ("pull_fraction", C.c_float), ("grid_blocks", C.c_uint32),
                 ("timeout_ms", C.c_double), ("collect_reach", C.c_int32),
                 ("detect_negative_cycle", C.c_int32), ("light_heavy", C.c_int32), ("trace", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("dense_fraction", C.c_float), ("reserved", C.c_int32 * 3)]
 
 
 class TraceEntry(C.Structure):

@@ -44,6 +44,7 @@ extern "C" void b2_sssp_opts_default(b2_sssp_opts* o) {
   o->detect_negative_cycle = 0;
   o->light_heavy = 1;
   o->trace = 0;
+  o->dense_fraction = 0.0f;
 }
 
 extern "C" b2_status b2_device_free(void* p) {

@@ -64,6 +64,8 @@ struct PhaseRec {
   uint32_t dinv;        // float bits of 1/width (float graphs)
   uint32_t dbase;       // distance key at which bucket dbase_b starts (0 until re-based)
   uint32_t dbase_b;
+  uint32_t dense;       // 0: read the frontier queue; kDenseNear / kDenseSlot: sweep the stamps
+  uint32_t fstamp;      // stamp value marking the frontier's vertices in a sweep
 };
 
 // One entry per executed phase when tracing is on (manager-written).
@@ -86,6 +88,17 @@ enum PhaseKind : uint32_t {
   kPhaseDone = 6,
   kPhaseLocal = 7,     // delta: block 0 alone runs small light sub-phases (bucket fusion)
   kPhasePull = 8,      // delta: heavy pass in the pull direction (unsettled vertices scan in-edges)
+};
+
+// How a delta-stepping relaxation phase finds its frontier.  A large near
+// frontier is the set of vertices whose push stamp equals the previous phase's
+// stamp; a large window-slot frontier is the set whose bucket stamp equals the
+// current bucket.  Sweeping those stamps in vertex order replaces random queue
+// order with ordered access to labels, row pointers and rows.
+enum DenseKind : uint32_t {
+  kDenseOff = 0,
+  kDenseNear = 1,
+  kDenseSlot = 2,
 };
 
 enum QueueId : uint32_t {

@@ -103,6 +103,7 @@ struct Params {
   uint32_t fusion;        // light frontiers up to this size run as a LOCAL phase (0: off)
   uint32_t adapt;         // ADDS: adjust the bucket width at window boundaries
   uint32_t adapt_cap;     // ADDS: frontier entries the grid takes per phase (utilization base)
+  uint32_t dense_min;     // delta: near / slot frontiers of at least this many entries are swept
 };
 
 // ---------------------------------------------------------------------------
@@ -177,13 +178,16 @@ __device__ __forceinline__ void store_rec(Control* c, const PhaseRec& r) {
 // happen when a buffer passes half full and at the end of every phase.
 constexpr int kWarpsPerBlock = kThreads / 32;
 constexpr uint32_t kNearBuf = 256, kFarBuf = 256, kSlotBuf = 256, kMemBuf = 128;
-constexpr uint32_t kStageWords = kNearBuf + kFarBuf + 2 * kSlotBuf + kMemBuf;
+constexpr uint32_t kDenseSpan = 256;   // vertices per sweep work item (8 per lane)
+constexpr uint32_t kListBuf = kDenseSpan + 32;   // one span's vertices + fewer than 32 carried
+constexpr uint32_t kStageWords = kNearBuf + kFarBuf + 2 * kSlotBuf + kMemBuf + kListBuf;
 constexpr size_t kStageBytes = (size_t)kWarpsPerBlock * kStageWords * 4;
 struct WarpQ {
   uint32_t* nearb;   // kNearBuf vertex ids
   uint32_t* farb;    // kFarBuf
   uint32_t* slotb;   // kSlotBuf (vertex, slot) pairs as 2 words
   uint32_t* memb;    // kMemBuf
+  uint32_t* listb;   // kListBuf frontier vertices found by a sweep
   uint32_t nn = 0, nf = 0, ns = 0, nm = 0;
 };
 
@@ -502,20 +506,17 @@ __device__ __forceinline__ void hub_chunk(const Params& P, const PhaseRec& R, ui
   }
 }
 
-// One frontier chunk: entries [base, base + 32) of the frontier queue.
+// Expand up to 32 frontier vertices, one per lane (`present` lanes hold one).
 template <class W, bool PRED, int MODE>
-__device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& R, uint32_t base, Tally& t) {
-  const uint32_t* F = queue_ptr(P, R.fq);
-  const uint32_t cnt = R.fcount;
+__device__ __forceinline__ void expand_vertices(const Params& P, const PhaseRec& R, uint32_t v, bool present,
+                                                Tally& t) {
   const uint32_t lane = lane_id();
   Control* c = P.ctl;
   const bool members = MODE == kModeDelta && P.lightcnt && !R.heavy;
-  const uint32_t i = base + lane;
-  uint32_t v = 0, du = kInfKey;
+  uint32_t du = kInfKey;
   uint64_t lo = 0, hi = 0, row_end = 0;
   bool valid = false, has_heavy = false;
-  if (i < cnt) {
-    v = ldcg(F + i);
+  if (present) {
     du = src_key<W, PRED, MODE>(P, v);
     valid = du != kInfKey;
     if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
@@ -608,41 +609,123 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
   }
 }
 
-// A relaxation phase: hub chunks of the previous phase, then 32-vertex
-// frontier chunks, handed out one at a time from a phase counter so no warp
-// idles while another holds a long tail.
+// Append the frontier's vertices among [span * 256, span * 256 + 256) (stamp
+// == R.fstamp; 8 consecutive vertices per lane) to the warp's list after its
+// `carry` entries, in vertex order; returns the new length.  A stamp that
+// changes under the sweep belongs to a vertex improved again in this phase: it
+// sits in this phase's near queue and is expanded next phase with its newer
+// label.
+__device__ __forceinline__ uint32_t sweep_span(const Params& P, const PhaseRec& R, uint32_t span, uint32_t* list,
+                                               uint32_t carry) {
+  const uint32_t lane = lane_id();
+  const uint32_t* S = R.dense == kDenseSlot ? P.bstamp : P.pstamp;
+  const uint32_t v0 = span * kDenseSpan + 8u * lane;
+  uint32_t m = 0;
+  if ((uint64_t)v0 + 8 <= P.n) {
+    const uint4 a = __ldcg(reinterpret_cast<const uint4*>(S + v0));
+    const uint4 b = __ldcg(reinterpret_cast<const uint4*>(S + v0 + 4));
+    m = (a.x == R.fstamp ? 1u : 0u) | (a.y == R.fstamp ? 2u : 0u) | (a.z == R.fstamp ? 4u : 0u) |
+        (a.w == R.fstamp ? 8u : 0u) | (b.x == R.fstamp ? 16u : 0u) | (b.y == R.fstamp ? 32u : 0u) |
+        (b.z == R.fstamp ? 64u : 0u) | (b.w == R.fstamp ? 128u : 0u);
+  } else {
+    for (uint32_t k = 0; k < 8 && v0 + k < P.n; ++k) m |= (ldcg(S + v0 + k) == R.fstamp ? 1u : 0u) << k;
+  }
+  const uint32_t cnt = __popc(m);
+  const uint32_t incl = warp_incl_scan(cnt);
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0) return carry;
+  __syncwarp();   // the previous item's reads of the list are done
+  uint32_t pos = carry + incl - cnt;
+  while (m) {
+    const uint32_t k = __ffs(m) - 1;
+    m &= m - 1;
+    list[pos++] = v0 + k;
+  }
+  __syncwarp();
+  return carry + total;
+}
+
+// One frontier work item: entries [32 item, 32 item + 32) of the frontier
+// queue, or the frontier vertices of sweep span `item`.  A sweep expands only
+// whole groups of 32 and carries the rest (`carry`) into the warp's next
+// item, so sparse spans do not run lanes idle; `flush` expands the carried
+// rest at the end of the phase.
+template <class W, bool PRED, int MODE>
+__device__ __forceinline__ void frontier_item(const Params& P, const PhaseRec& R, uint32_t item, bool dense,
+                                              bool flush, uint32_t& carry, Tally& t) {
+  const uint32_t lane = lane_id();
+  const uint32_t base = item * 32;
+  uint32_t total, limit;
+  if (dense) {
+    total = flush ? carry : sweep_span(P, R, item, t.q.listb, carry);
+    limit = flush ? total : (total & ~31u);
+  } else {
+    total = min(32u, R.fcount - base);
+    limit = total;
+  }
+  for (uint32_t j0 = 0; j0 < limit; j0 += 32) {
+    const bool present = j0 + lane < total;
+    uint32_t v = 0;
+    if (present) v = dense ? t.q.listb[j0 + lane] : ldcg(queue_ptr(P, R.fq) + base + lane);
+    expand_vertices<W, PRED, MODE>(P, R, v, present, t);
+  }
+  if (dense) {
+    const uint32_t rest = total - limit;   // < 32
+    if (limit && rest) {
+      __syncwarp();
+      const uint32_t v = lane < rest ? t.q.listb[limit + lane] : 0u;
+      __syncwarp();
+      if (lane < rest) t.q.listb[lane] = v;
+      __syncwarp();
+    }
+    carry = rest;
+  }
+}
+
+// One frontier chunk of the queue (block-local sub-phases).
+template <class W, bool PRED, int MODE>
+__device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& R, uint32_t base, Tally& t) {
+  uint32_t carry = 0;
+  frontier_item<W, PRED, MODE>(P, R, base / 32, false, false, carry, t);
+}
+
 constexpr uint32_t kHubGrab = B2_HUB_GRAB;   // hub chunks per work item
 
 // A relaxation phase: hub chunks of the previous phase, then 32-vertex
-// frontier chunks.  Items are first dealt round-robin to the warps (3/4 of
-// them, no atomics), the rest handed out one at a time from a phase counter
-// so no warp idles while another holds a long tail.
+// frontier chunks (or 256-vertex sweep items).  Items are first dealt
+// round-robin to the warps (3/4 of them, no atomics), the rest handed out one
+// at a time from a phase counter so no warp idles while another holds a long
+// tail.
 template <class W, bool PRED, int MODE>
 __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t nhub = min(R.hub_in_chunks, P.hub_cap);
   const uint32_t nhg = (nhub + kHubGrab - 1) / kHubGrab;
-  const uint32_t nfc = (R.fcount + 31) / 32;
+  const bool dense = MODE == kModeDelta && R.dense != kDenseOff;
+  const uint32_t nfc = dense ? (P.n + kDenseSpan - 1) / kDenseSpan : (R.fcount + 31) / 32;
   const uint32_t items = nhg + nfc;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t rounds = (items * B2_STATIC_NUM / 4) / nwarps;
   const uint32_t nstatic = rounds * nwarps;
   Control* c = P.ctl;
-  auto run = [&](uint32_t item) {
-    if (item < nhg) {
+  uint32_t carry = 0;   // swept vertices waiting in the warp's list
+  for (uint32_t r = 0;; ++r) {
+    uint32_t item = 0;
+    if (r < rounds) {
+      item = r * nwarps + gwarp;
+    } else {
+      if (lane_id() == 0) item = atomicAdd(&c->work_next, 1u);
+      item = __shfl_sync(0xffffffffu, item, 0) + nstatic;
+    }
+    const bool done = item >= items;
+    if (done && carry == 0) break;
+    if (!done && item < nhg) {
       const uint32_t h1 = min(nhub, (item + 1) * kHubGrab);
       for (uint32_t h = item * kHubGrab; h < h1; ++h) hub_chunk<W, PRED, MODE>(P, R, h, t);
     } else {
-      frontier_chunk<W, PRED, MODE>(P, R, (item - nhg) * 32, t);
+      frontier_item<W, PRED, MODE>(P, R, done ? 0u : item - nhg, dense, done, carry, t);
     }
-  };
-  for (uint32_t r = 0; r < rounds; ++r) run(r * nwarps + gwarp);
-  for (;;) {
-    uint32_t item = 0;
-    if (lane_id() == 0) item = atomicAdd(&c->work_next, 1u);
-    item = __shfl_sync(0xffffffffu, item, 0) + nstatic;
-    if (item >= items) break;
-    run(item);
+    if (done) break;
   }
   flush_all<MODE>(P, R, t.q, true);
 }
@@ -714,7 +797,7 @@ __device__ __forceinline__ void trace_phase(const Params& P, const PhaseRec& r, 
   const uint32_t i = vld(&c->trace_n);
   if (i >= kTraceCap) return;
   TraceEntry e;
-  e.kind = r.kind | (r.heavy ? 0x100u : 0u);
+  e.kind = r.kind | (r.heavy ? 0x100u : 0u) | (r.dense ? 0x200u : 0u);
   e.fcount = r.fcount;
   e.hub_chunks = r.hub_in_chunks;
   e.cur = tag;
@@ -864,11 +947,21 @@ __device__ void manager_bf(const Params& P) {
   store_rec(c, nx);
 }
 
+// A large near or slot frontier is found by a stamp sweep (see sweep_span).
+__device__ __forceinline__ void set_dense(const Params& P, PhaseRec& nx, uint32_t kind, uint32_t stamp) {
+  if (nx.kind == kPhaseProcess && nx.fcount >= P.dense_min) {
+    nx.dense = kind;
+    nx.fstamp = stamp;
+  }
+}
+
 __device__ void manager_delta(const Params& P) {
   Control* c = P.ctl;
   const PhaseRec r = load_rec(c);
   trace_phase(P, r, r.cur);
   PhaseRec nx = r;
+  nx.dense = kDenseOff;
+  nx.fstamp = 0u;
   nx.phase = r.phase + 1;
   nx.stamp = P.phase_base + (c->stamp_ctr++);
   c->phases = vld(&c->phases) + 1;
@@ -929,6 +1022,7 @@ __device__ void manager_delta(const Params& P) {
         nx.fcount = nn;
         nx.push_q = r.push_q ^ 1u;
         nx.hround = P.phase_base + nx.phase;
+        set_dense(P, nx, kDenseNear, r.stamp);
         store_rec(c, nx);
         return;
       }
@@ -939,6 +1033,8 @@ __device__ void manager_delta(const Params& P) {
         nx.fcount = nn;
         nx.push_q = r.push_q ^ 1u;
         if (hch == 0 && nn <= P.fusion && !vld(&c->fusion_off)) nx.kind = kPhaseLocal;
+        // (a LOCAL phase's last pushes carry a stamp drawn inside it: no sweep after one)
+        if (nn > 0 && r.kind != kPhaseLocal) set_dense(P, nx, kDenseNear, r.stamp);
         store_rec(c, nx);
         return;
       }
@@ -1004,6 +1100,7 @@ __device__ void manager_delta(const Params& P) {
     nx.fcount = cnts[found];
     nx.push_q = kQNear0;   // both near queues are empty at a bucket boundary
     if (nx.fcount <= P.fusion && !vld(&c->fusion_off)) nx.kind = kPhaseLocal;
+    set_dense(P, nx, kDenseSlot, nx.cur);
     store_rec(c, nx);
     return;
   }
@@ -1131,6 +1228,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
     t.q.farb = wb + kNearBuf;
     t.q.slotb = wb + kNearBuf + kFarBuf;
     t.q.memb = wb + kNearBuf + kFarBuf + 2 * kSlotBuf;
+    t.q.listb = t.q.memb + kMemBuf;
   }
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -1455,6 +1553,11 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     }
     P.max_iters = o.max_iters < 0 ? 0xFFFFFFFFu : (uint32_t)o.max_iters;
     P.fusion = o.fusion_threshold;
+    // stamp sweeps pay on low-degree graphs; on skewed ones the vertex order
+    // bunches heavy rows into the same sweep items (a long tail per phase)
+    const float dfrac = o.dense_fraction != 0.0f ? o.dense_fraction : (g->max_degree <= 64 ? 1.0f / 16.0f : -1.0f);
+    P.dense_min = dfrac > 0.0f ? (uint32_t)std::min(4294967295.0, std::max(1.0, std::ceil((double)dfrac * g->n)))
+                               : 0xFFFFFFFFu;
     if (adds) {
       int dev = 0, sms = 0;
       cudaGetDevice(&dev);

@@ -435,3 +435,47 @@ def test_pull_switch_point(b2, orc, cuda):
     assert gg.info()["device_bytes"] == before                   # no incoming CSR for a sparse grid
     g.close()
     gg.close()
+
+
+@pytest.mark.parametrize("weight", ["u32", "f32"])
+def test_stamp_sweep_matches_queue(b2, orc, cuda, weight):
+    """Frontiers found by sweeping the push / bucket stamps (forced on every
+    phase with a tiny threshold) give the queue path's words exactly:
+    distances, predecessors and bucket counts, for delta and ADDS, on a grid,
+    an ER graph and a degree-ordered RMAT graph.  (Block-local sub-phases,
+    which ADDS uses for small frontiers on low-degree graphs, always read
+    their queues; a threshold of one keeps them out of the way.)"""
+    graphs = [b2.gen_grid(60, 70, 0.02, seed=51), b2.gen_er(3000, 24000, 1, 1000, seed=52),
+              b2.gen_rmat(13, 16, seed=53)]
+    for k, hg in enumerate(graphs):
+        w = hg.weights if weight == "u32" else hg.fweights
+        g = b2.Graph.from_host(hg, weight)
+        if k == 2:
+            g.set_degree_order()
+        for method in ("delta", "adds"):
+            for s in (0, hg.n // 2):
+                ref = orc.dijkstra(hg.rowptr, hg.colind, w, s)
+                dq, pq, sq = g.sssp(s, method=method, pred=True, dense_fraction=-1.0, fusion_threshold=1)
+                dd, pd, sd = g.sssp(s, method=method, pred=True, dense_fraction=1e-9, fusion_threshold=1,
+                                    trace=1)
+                assert any(e["kind"].endswith("-dense") for e in g.trace())
+                assert np.array_equal(_raw(dd, weight), ref)
+                assert np.array_equal(_raw(dq, weight), ref)
+                assert np.array_equal(pd.cpu().numpy(), pq.cpu().numpy())
+                assert sd["iterations_used"] == sq["iterations_used"]
+                d2, _, _ = g.sssp(s, method=method, dense_fraction=1e-9)      # no predecessors
+                assert np.array_equal(_raw(d2, weight), ref)
+        g.close()
+
+
+def test_stamp_sweep_default_follows_degree(b2, cuda):
+    """By default a low-degree grid sweeps its large frontiers and a skewed
+    RMAT graph keeps reading its queues."""
+    grid = b2.Graph.from_host(b2.gen_grid(128, 128, 0.02, seed=54), "u32")
+    grid.sssp(0, trace=1)
+    assert any(e["kind"].endswith("-dense") for e in grid.trace())
+    rm = b2.Graph.from_host(b2.gen_rmat(14, 16, seed=55), "u32")
+    rm.sssp(0, trace=1)
+    assert not any(e["kind"].endswith("-dense") for e in rm.trace())
+    grid.close()
+    rm.close()
