@@ -70,9 +70,10 @@ def load_peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profile_traffic() -> float | None:
+def profile_traffic(graph: str = "rmat") -> float | None:
     """dram bytes per launch of the persistent kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "sssp_delta_rmat24.md")
+    name = "sssp_delta_rmat24.md" if graph == "rmat" else "sssp_delta_grid4096.md"
+    p = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -384,7 +385,7 @@ def main():
                 "note": "graph resident; source id passed by value; distances copied to pinned host"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": profile_traffic() if args.graph == "rmat" else None,
+                     "frac": achieved / peak, "traffic": profile_traffic(args.graph),
                      "peak_kind": peak_kind,
                      "kernel": "k_sssp<WU32,false,kModeDelta>",
                      "bytes_alg_per_launch": bytes_alg / args.steps,
