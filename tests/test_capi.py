@@ -36,6 +36,7 @@ def test_status_strings_and_defaults(b2):
         assert _lib.status_string(s) and "unknown" not in _lib.status_string(s)
     o = _lib.default_opts()
     assert o.max_iters == -1 and o.delta_scale == 16.0 and o.timeout_ms == 20000.0 and o.hub_degree == 256
+    assert o.pull_fraction == 8.0 and o.dense_fraction == 0.0 and o.light_heavy == 1   # 0: by graph degree
 
 
 def test_generators_deterministic_and_thread_independent(b2, monkeypatch):
