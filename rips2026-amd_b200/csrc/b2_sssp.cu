@@ -95,6 +95,7 @@ struct Params {
   int32_t* out_pred;
   uint32_t dist_is_out;   // `dist` aliases out_dist (no separate label buffer)
   const uint32_t* perm;   // degree-ordered graph: internal -> input id of every output slot (else null)
+  const uint32_t* inv;    // degree-ordered graph: input -> internal id (else null)
   const uint64_t* __restrict__ in_rowptr;   // incoming CSR for the pull heavy pass (null: push only)
   const uint2* __restrict__ in_edges;       // (source, weight bits), rows sorted by weight
   const uint32_t* __restrict__ in_lightcnt; // light prefix of each incoming row
@@ -1326,10 +1327,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
     } else if (R.kind == kPhaseFinal) {
       const typename L::T* srcl =
           (const typename L::T*)((MODE == kModeBF && R.aux == 1u) ? P.dist_cur : P.dist);
-      for (size_t v = tid; v < P.n; v += stride) {
+      // in output order: a degree-ordered graph gathers each slot's label
+      // (mostly L2-resident) instead of scattering 4-byte writes
+      for (size_t o = tid; o < P.n; o += stride) {
+        const size_t v = P.inv ? (size_t)__ldg(P.inv + o) : o;   // internal id of output slot o
         const typename L::T wv = ldcg(srcl + v);
         const uint32_t k = L::key(wv);
-        const size_t o = P.perm ? (size_t)__ldg(P.perm + v) : v;   // input id of internal vertex v
         if (W::kFloat) {
           ((float*)P.out_dist)[o] = (k == kInfKey) ? __uint_as_float(0x7f800000u) : key_to_f32(k);
         } else if (!P.dist_is_out || (const void*)srcl != P.out_dist) {
@@ -1503,6 +1506,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   P.n = (uint32_t)g->n;
   P.source = internal_id(g, source);
   P.perm = g->perm;
+  P.inv = g->perm ? g->inv : nullptr;
   P.rowptr = g->rowptr;
   P.edges = g->edges;
   P.pstamp = w.pstamp;
