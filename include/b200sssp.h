@@ -28,6 +28,10 @@
  *   b2_minplus_spgemm_i32 <- (int32 twin of the above)
  *   b2_delta_heuristic    <- choose_initial_delta (Charlotte_oneshot/sssp_hip.cpp:59-81),
  *                            estimate_initial_delta (hip_adds_sssp.cpp:1080-1127)
+ *   b2_dimacs_read, b2_dimacs_to_csrbin <- load_dimacs_gr_as_incoming_csr and the converter main
+ *                            (HIP_kernel/bellman_ford/src/gr_to_csr.cpp:124-326)
+ *   b2_lonestar_read/write <- CSRGraph::readFromGR
+ *                            (faster_GPU_algo/Charlotte_ADS_Float_Attempt/csr_graph.cpp:153-291)
  *   b2_csrbin_read/write  <- RIPSCSR1 writer/loaders (HIP_kernel/bellman_ford/src/gr_to_csr.cpp:34-57,
  *                            :243-278; tests/big_test.cpp:160-276)
  */
@@ -430,6 +434,28 @@ b2_status b2_host_csr_transpose(const b2_host_csr* in, b2_host_csr* out);
 b2_status b2_csrbin_write(const char* path, int64_t n, int64_t nnz, const int64_t* rowptr,
                           const int32_t* colind, const float* values);
 b2_status b2_csrbin_read(const char* path, b2_host_csr* out);
+
+/* DIMACS shortest-path text graph (.gr: "c" comments, "p <kind> n m", "a u v w" with 1-based
+ * ids) as an INCOMING CSR with float weights, read under the rules of the reference's converter
+ * (HIP_kernel/bellman_ford/src/gr_to_csr.cpp:124-230): columns ascending in each row, repeated
+ * arcs reduced to their smallest weight, self-loops kept, unknown line kinds ignored.  Errors:
+ * B2_INVALID_ARGUMENT (unreadable file, bad or missing problem line, arc before it, malformed
+ * arc), B2_INVALID_INDEX (endpoint outside [1, n]), B2_INVALID_WEIGHT (non-finite weight).
+ * declared_arcs / loaded_arcs (nullable): the problem line's m and the arc lines read. */
+b2_status b2_dimacs_read(const char* path, b2_host_csr* out, int64_t* declared_arcs, int64_t* loaded_arcs);
+/* The reference converter in one call (gr_to_csr.cpp:232-326): DIMACS .gr -> RIPSCSR1 .csrbin,
+ * byte-identical to its output.  nnz_out (nullable): arcs after duplicate reduction. */
+b2_status b2_dimacs_to_csrbin(const char* gr_path, const char* csrbin_path, int64_t* nnz_out);
+/* Galois / Lonestar binary .gr, version 1, as the ADDS port loads it
+ * (HIP_kernel/faster_GPU_algo/Charlotte_ADS_Float_Attempt/csr_graph.cpp:153-291): OUTGOING CSR;
+ * no edge data = weight 1; 4-byte edge data are floats when data_is_float (the port's reading:
+ * finite and >= 0 required, else B2_INVALID_WEIGHT) or uint32 otherwise.  Bad header or
+ * truncated file: B2_INVALID_ARGUMENT; offsets not monotone / not ending at m:
+ * B2_INVALID_ROWPTR; destination >= n: B2_INVALID_INDEX. */
+b2_status b2_lonestar_read(const char* path, int32_t data_is_float, b2_host_csr* out);
+/* Write an OUTGOING CSR as Lonestar .gr version 1 with 4-byte edge data (fweights when
+ * data_is_float, else weights). */
+b2_status b2_lonestar_write(const char* path, const b2_host_csr* g, int32_t data_is_float);
 
 #ifdef __cplusplus
 }

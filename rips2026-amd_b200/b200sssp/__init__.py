@@ -18,7 +18,8 @@ from . import _lib
 from ._lib import B2Error, LibraryMissing, check, default_opts, lib  # noqa: F401
 
 __all__ = ["HostGraph", "Graph", "gen_er", "gen_rmat", "gen_grid", "B2Error", "LibraryMissing",
-           "minplus_gemm", "apsp", "minplus_spgemm", "csrbin_read", "csrbin_write"]
+           "minplus_gemm", "apsp", "minplus_spgemm", "csrbin_read", "csrbin_write", "dimacs_read",
+           "dimacs_to_csrbin", "lonestar_read", "lonestar_write"]
 
 
 # ---------------------------------------------------------------------------
@@ -114,6 +115,38 @@ def csrbin_read(path: str) -> HostGraph:
     h = _lib.HostCSR()
     check(lib().b2_csrbin_read(path.encode(), C.byref(h)), "csrbin_read")
     return _from_hostcsr(h, "incoming")
+
+
+def dimacs_read(path: str) -> tuple[HostGraph, int, int]:
+    """DIMACS shortest-path .gr text as an INCOMING float CSR, read like the
+    reference's gr_to_csr converter; returns (graph, declared arcs, arc lines read)."""
+    h = _lib.HostCSR()
+    declared, loaded = C.c_int64(), C.c_int64()
+    check(lib().b2_dimacs_read(path.encode(), C.byref(h), C.byref(declared), C.byref(loaded)), "dimacs_read")
+    return _from_hostcsr(h, "incoming"), declared.value, loaded.value
+
+
+def dimacs_to_csrbin(gr_path: str, csrbin_path: str) -> int:
+    """The reference converter: DIMACS .gr -> RIPSCSR1 .csrbin; returns the arcs kept."""
+    nnz = C.c_int64()
+    check(lib().b2_dimacs_to_csrbin(gr_path.encode(), csrbin_path.encode(), C.byref(nnz)), "dimacs_to_csrbin")
+    return nnz.value
+
+
+def lonestar_read(path: str, float_weights: bool = True) -> HostGraph:
+    """Galois / Lonestar binary .gr (version 1) as an OUTGOING CSR; 4-byte edge data
+    read as float (the ADDS port's reading) or as uint32."""
+    h = _lib.HostCSR()
+    check(lib().b2_lonestar_read(path.encode(), 1 if float_weights else 0, C.byref(h)), "lonestar_read")
+    return _from_hostcsr(h, "outgoing")
+
+
+def lonestar_write(path: str, g: HostGraph, float_weights: bool = True) -> None:
+    """Write an OUTGOING CSR as Lonestar .gr version 1 (fweights or uint32 weights)."""
+    if g.orientation != "outgoing":
+        raise ValueError("Lonestar .gr stores outgoing CSR")
+    h = _to_hostcsr(g)
+    check(lib().b2_lonestar_write(path.encode(), C.byref(h), 1 if float_weights else 0), "lonestar_write")
 
 
 # ---------------------------------------------------------------------------

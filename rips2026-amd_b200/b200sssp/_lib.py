@@ -144,6 +144,10 @@ _SIGS = {
     "b2_host_csr_transpose": (C.c_int, [C.POINTER(HostCSR), C.POINTER(HostCSR)]),
     "b2_csrbin_write": (C.c_int, [C.c_char_p, C.c_int64, C.c_int64, _P, _P, _P]),
     "b2_csrbin_read": (C.c_int, [C.c_char_p, C.POINTER(HostCSR)]),
+    "b2_dimacs_read": (C.c_int, [C.c_char_p, C.POINTER(HostCSR), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "b2_dimacs_to_csrbin": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int64)]),
+    "b2_lonestar_read": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(HostCSR)]),
+    "b2_lonestar_write": (C.c_int, [C.c_char_p, C.POINTER(HostCSR), C.c_int32]),
 }
 
 _lib = None
