@@ -24,6 +24,9 @@ Fixtures written:
                     device="cpu") on seeded graphs, several deltas.
   tiny_gr.json      the five-vertex graph of Charlotte_ADS_Float_Attempt/tools/make_tiny_gr.py
                     and its expected distances (check_tiny_output.py:10).
+  tiny.gr           that graph as the reference's own tool writes it (Lonestar binary .gr),
+                    with tiny_gr.json's expected distances read from check_tiny_output.py.
+                    `python tests/golden/make_golden.py REF --only tiny` regenerates these two.
 """
 from __future__ import annotations
 
@@ -249,13 +252,36 @@ def main(ref: str) -> None:
         bk[f"b{t}/dist"], bk[f"b{t}/delta"] = d, np.array([delta], np.float32)
     np.savez_compressed(os.path.join(HERE, "bucketed.npz"), **bk)
 
-    # ---------------------------------------------------------------- tiny .gr
-    tiny = {"n": 5, "out_rowptr": [0, 2, 4, 5, 5, 5], "out_colind": [1, 2, 2, 3, 3],
-            "weights": [1.0, 4.0, 2.0, 5.0, 1.0], "source": 0, "expected": [0.0, 1.0, 3.0, 4.0, None]}
-    with open(os.path.join(HERE, "tiny_gr.json"), "w") as f:
-        json.dump(tiny, f)
+    tiny_fixtures(ref)
     print("fixtures written to", HERE)
 
 
+def tiny_fixtures(ref: str) -> None:
+    """The reference's tiny Lonestar graph, written by its own make_tiny_gr.py, and the
+    expected distances of its check_tiny_output.py."""
+    import runpy
+    import subprocess
+    tools = os.path.join(ref, "HIP_kernel", "faster_GPU_algo", "Charlotte_ADS_Float_Attempt", "tools")
+    gr = os.path.join(HERE, "tiny.gr")
+    subprocess.run([sys.executable, os.path.join(tools, "make_tiny_gr.py"), gr], check=True)
+    expected = runpy.run_path(os.path.join(tools, "check_tiny_output.py"), run_name="golden")["EXPECTED"]
+    raw = open(gr, "rb").read()
+    _, _, n, m = np.frombuffer(raw[:32], np.uint64).tolist()
+    ends = np.frombuffer(raw[32:32 + 8 * n], np.uint64)
+    dst = np.frombuffer(raw[32 + 8 * n:32 + 8 * n + 4 * m], np.uint32)
+    off = 32 + 8 * n + 4 * m + (4 if m % 2 else 0)
+    w = np.frombuffer(raw[off:off + 4 * m], np.float32)
+    tiny = {"n": int(n), "out_rowptr": [0] + ends.astype(int).tolist(), "out_colind": dst.astype(int).tolist(),
+            "weights": w.astype(float).tolist(), "source": 0,
+            "expected": [None if np.isinf(expected[v]) else float(expected[v]) for v in range(int(n))]}
+    with open(os.path.join(HERE, "tiny_gr.json"), "w") as f:
+        json.dump(tiny, f)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if a != "--only" and a != "tiny"]
+    ref_dir = args[0] if args else "/root/reference"
+    if "--only" in sys.argv:
+        tiny_fixtures(ref_dir)
+    else:
+        main(ref_dir)

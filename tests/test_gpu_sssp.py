@@ -479,3 +479,19 @@ def test_stamp_sweep_default_follows_degree(b2, cuda):
     assert not any(e["kind"].endswith("-dense") for e in rm.trace())
     grid.close()
     rm.close()
+
+
+def test_reference_tiny_lonestar_known_answer(b2, cuda):
+    """The reference's tiny Lonestar graph (tests/golden/tiny.gr, written by its
+    make_tiny_gr.py) solved from the file: every method gives the distances of
+    its check_tiny_output.py."""
+    import json
+    import os
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    t = json.load(open(os.path.join(golden, "tiny_gr.json")))
+    exp = np.array([np.inf if x is None else x for x in t["expected"]], np.float32)
+    g = b2.Graph.from_host(b2.lonestar_read(os.path.join(golden, "tiny.gr")), "f32")
+    for method in ("bf", "delta", "adds"):
+        d, _, st = g.sssp(t["source"], method=method)
+        assert np.array_equal(_np(d), exp), method
+    g.close()

@@ -182,3 +182,22 @@ def test_dimacs_to_lonestar_round_trip(tmp_path, b2):
     back = b2.lonestar_read(str(f)).transpose()
     assert np.array_equal(back.rowptr, g.rowptr) and np.array_equal(back.colind, g.colind)
     assert np.array_equal(back.fweights, g.fweights)
+
+
+def test_reference_tiny_lonestar_file(b2, orc):
+    """tests/golden/tiny.gr was written by the reference's own make_tiny_gr.py
+    (tests/golden/make_golden.py): the reader gives its graph, the writer its
+    bytes, and the oracle its expected distances (check_tiny_output.py:10)."""
+    import json
+    golden = os.path.join(ROOT, "tests", "golden")
+    t = json.load(open(os.path.join(golden, "tiny_gr.json")))
+    g = b2.lonestar_read(os.path.join(golden, "tiny.gr"))
+    assert g.n == t["n"] and g.rowptr.tolist() == t["out_rowptr"] and g.colind.tolist() == t["out_colind"]
+    assert g.fweights.tolist() == t["weights"]
+    exp = np.array([np.inf if x is None else x for x in t["expected"]], np.float32)
+    assert np.array_equal(orc.dijkstra(g.rowptr, g.colind, g.fweights, t["source"]), exp)
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "tiny.gr")
+        b2.lonestar_write(out, g)
+        assert open(out, "rb").read() == open(os.path.join(golden, "tiny.gr"), "rb").read()
