@@ -554,6 +554,9 @@ struct Lane {
   // The launch sequence of a batch (reset the query counter, run the teams)
   // as an instantiated CUDA graph per team kind; each batch updates the
   // kernel node's grid and arguments and replays it.
+  // (the source graph stays alive with its instantiation: kernel-node
+  // updates name a node of the graph the executable was made from)
+  cudaGraph_t gsrc[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   cudaGraphNode_t knode[2] = {nullptr, nullptr};
   bool graph_failed = false;      // graph API refused: launch directly
@@ -589,11 +592,13 @@ cudaError_t launch_batch_graph(Lane& ln, bool big, uint32_t grid, uint32_t nq, u
     }
     if (e == cudaSuccess) e = cudaGraphAddKernelNode(&ln.knode[k], graph, &mnode, 1, &kp);
     if (e == cudaSuccess) e = cudaGraphInstantiate(&ln.gexec[k], graph, 0);
-    if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
       ln.gexec[k] = nullptr;
+      ln.knode[k] = nullptr;
       return e;
     }
+    ln.gsrc[k] = graph;
   } else {
     e = cudaGraphExecKernelNodeSetParams(ln.gexec[k], ln.knode[k], &kp);
     if (e != cudaSuccess) return e;
@@ -914,8 +919,10 @@ extern "C" b2_status b2_server_destroy(b2_server s) {
   for (auto& ln : s->lanes)
     if (ln.st) cudaStreamSynchronize(ln.st);
   for (auto& ln : s->lanes) {
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 2; ++k) {
       if (ln.gexec[k]) cudaGraphExecDestroy(ln.gexec[k]);
+      if (ln.gsrc[k]) cudaGraphDestroy(ln.gsrc[k]);
+    }
     if (ln.st) cudaStreamDestroy(ln.st);
     if (ln.done) cudaEventDestroy(ln.done);
     cudaFree(ln.d_next);
