@@ -224,7 +224,9 @@ b2_status b2_sssp_bf_dense(const float* d_adj, int32_t n, uint32_t source, float
  * C[i,j] = min_k A[i,k] + B[k,j], row-major with leading dimensions.
  * f32: NaN candidates are ignored, empty min = +inf.
  * i32: inputs must lie in [-2^30, 2^30-1]; C is clamped to <= INT32_MAX/2
- *      (1073741823, the "missing" sentinel).  Asynchronous on `stream`. */
+ *      (1073741823, the "missing" sentinel).  Asynchronous on `stream`: the
+ * return value covers the launch only; b2_minplus_status reports a product
+ * whose bounded wait gave up. */
 b2_status b2_minplus_gemm_f32(const float* dA, const float* dB, float* dC, int32_t M,
                               int32_t N, int32_t K, int32_t lda, int32_t ldb, int32_t ldc,
                               b2_stream stream);
@@ -236,6 +238,13 @@ b2_status b2_minplus_gemm_i32(const int32_t* dA, const int32_t* dB, int32_t* dC,
  * nothing.  *squarings_out = products computed. */
 b2_status b2_apsp_f32(float* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
 b2_status b2_apsp_i32(int32_t* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
+/* Waits for `stream`, then returns B2_TIMEOUT if a min-plus product launched
+ * on this device since the last b2_minplus_gemm_* / b2_apsp_* call began had
+ * a bounded shared-memory wait give up (its output is then not valid), else
+ * B2_SUCCESS.  The record is one word per device, cleared in stream order by
+ * every GEMM and APSP call: products that overlap on different streams share
+ * it.  No counterpart in the reference (its waits are unbounded). */
+b2_status b2_minplus_status(b2_stream stream);
 /* b2_apsp_f32 without any device allocation, for callers that cannot call
  * cudaMalloc while they run (a plugin whose host owns the device memory pool,
  * a serving loop with a fixed memory budget).  No counterpart in the
@@ -243,8 +252,10 @@ b2_status b2_apsp_i32(int32_t* d_D, int32_t N, b2_stream stream, int32_t* squari
  * (larger N returns B2_NOT_SUPPORTED); each GPU that loads the library holds
  * that array until exit.  All calls on a device share it: calls that overlap
  * on the GPU race and must be serialized by the caller.  The first call on a
- * device resolves the array's device address; make it before any stream
- * capture. */
+ * device resolves the array's device address (cudaGetSymbolAddress) with that
+ * device current.  Every call synchronizes `stream` after each squaring (it
+ * reads the change flag on the host), so no call may be made on a stream that
+ * is being captured. */
 b2_status b2_apsp_f32_noalloc(float* d_D, int32_t N, b2_stream stream, int32_t* squarings_out);
 /* Sustained (min,+) pairs per second of this GPU's CUDA cores, measured by a
  * register-only kernel of the same instruction mix as the GEMM inner loop

@@ -104,6 +104,7 @@ _SIGS = {
     "b2_apsp_f32": (C.c_int, [_P, C.c_int32, _P, C.POINTER(C.c_int32)]),
     "b2_apsp_i32": (C.c_int, [_P, C.c_int32, _P, C.POINTER(C.c_int32)]),
     "b2_apsp_f32_noalloc": (C.c_int, [_P, C.c_int32, _P, C.POINTER(C.c_int32)]),
+    "b2_minplus_status": (C.c_int, [_P]),
     "b2_minplus_calibrate": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
     "b2_minplus_spgemm_f32": (C.c_int, [C.POINTER(CSR), C.POINTER(CSR), C.POINTER(_P), C.POINTER(_P),
                                         C.POINTER(_P), C.POINTER(C.c_int64), _P]),

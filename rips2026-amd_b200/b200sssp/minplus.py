@@ -29,7 +29,11 @@ def _sp(stream):
         stream if isinstance(stream, int) else stream.cuda_stream)
 
 
-def minplus_gemm(A, B, out=None, stream=None):
+def minplus_gemm(A, B, out=None, stream=None, check_status: bool = True):
+    """C = A (min,+) B on the GPU.  The product is asynchronous on `stream`;
+    with check_status (default) the call waits for it and raises B2Error
+    (B2_TIMEOUT) if one of its bounded shared-memory waits gave up.  Callers
+    issuing many products can pass False and call status(stream) once."""
     torch = _torch()
     if A.dtype != B.dtype or A.dim() != 2 or B.dim() != 2 or A.shape[1] != B.shape[0]:
         raise ValueError("A (MxK) and B (KxN) must be 2-D with matching inner size and dtype")
@@ -44,7 +48,15 @@ def minplus_gemm(A, B, out=None, stream=None):
         raise TypeError("float32 or int32 operands required")
     check(fn(C.c_void_p(A.data_ptr()), C.c_void_p(B.data_ptr()), C.c_void_p(out.data_ptr()), M, N, K,
              A.stride(0), B.stride(0), out.stride(0), C.c_void_p(_sp(stream))), "minplus_gemm")
+    if check_status:
+        status(stream)
     return out
+
+
+def status(stream=None) -> None:
+    """Wait for `stream`; raise B2Error if a min-plus product issued since the
+    last GEMM / APSP call began gave up a bounded wait (b2_minplus_status)."""
+    check(lib().b2_minplus_status(C.c_void_p(_sp(stream))), "minplus_status")
 
 
 def apsp(D, stream=None) -> int:

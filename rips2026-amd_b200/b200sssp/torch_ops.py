@@ -7,6 +7,10 @@ custom operators on CUDA tensors (importing this module registers them).
       INCOMING CSR (row v, column u = w(u -> v)), float32 or int32 weights; max_iters < 0
       means n - 1.  Returns (dist, pred int64 (-1 = none), iterations_used, converged,
       has_negative_cycle), with the reference's extra relaxation round for the cycle check.
+      float32 weights may be negative (the reference's float64 rules, negative cycles
+      included) and give float32 distances.  int32 weights are solved as exact unsigned
+      integers and give int32 distances (0xFFFFFFFF bits = unreachable); they must be
+      nonnegative (a negative one raises ValueError: pass float32 values for those).
   torch.ops.b200sssp.bucketted_bellman_ford(rowptr, col, weight, source, num_nodes, delta=1.0)
       <- bucketted_bellman_ford (pytorch_testing/bellman_ford_attempts/bucketed_bellman_ford:1-71).
       OUTGOING CSR, float32 weights; delta-stepping with bucket width `delta`; returns dist.
@@ -39,7 +43,15 @@ def _stream():
 def sssp_min_plus_bellman_ford(rowptr: torch.Tensor, colind: torch.Tensor, values: torch.Tensor, source: int,
                                max_iters: int = -1) -> tuple[torch.Tensor, torch.Tensor, int, bool, bool]:
     _need_cuda(rowptr, colind, values)
-    g = Graph.from_arrays(rowptr, colind, values, orientation="incoming", stream=_stream())
+    if values.dtype == torch.float32:
+        weight = "f32"
+    elif values.dtype == torch.int32:
+        if values.numel() and bool((values < 0).any()):
+            raise ValueError("negative int32 weights: pass float32 values for negative weights")
+        weight = "u32"
+    else:
+        raise TypeError("values must be float32 or int32")
+    g = Graph.from_arrays(rowptr, colind, values, orientation="incoming", weight=weight, stream=_stream())
     try:
         dist, pred, st = g.sssp(int(source), method="bf", pred=True, max_iters=int(max_iters),
                                 detect_negative_cycle=1, stream=_stream())
@@ -52,7 +64,8 @@ def sssp_min_plus_bellman_ford(rowptr: torch.Tensor, colind: torch.Tensor, value
 @sssp_min_plus_bellman_ford.register_fake
 def _(rowptr, colind, values, source, max_iters=-1):
     n = rowptr.shape[0] - 1
-    return (values.new_empty(n), rowptr.new_empty(n, dtype=torch.int64), 0, False, False)
+    dt = torch.float32 if values.dtype == torch.float32 else torch.int32
+    return (values.new_empty(n, dtype=dt), rowptr.new_empty(n, dtype=torch.int64), 0, False, False)
 
 
 @torch.library.custom_op("b200sssp::bucketted_bellman_ford", mutates_args=())

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 
 #include "b2_common.cuh"
 #include "b2_internal.hpp"
@@ -38,7 +39,12 @@ constexpr int A_TILE = BM * BK;   // elements
 constexpr int B_TILE = BK * BN;
 constexpr int kMissing = 1073741823;
 
-__device__ uint32_t g_mp_error;   // bounded mbarrier wait expired (sticky)
+// Set by a bounded mbarrier wait that gave up.  One word per device: every
+// product clears it in stream order before its launch (clear_mp_error), APSP
+// reads it back after its last product, and b2_minplus_status reads it for
+// the asynchronous GEMM.  Products that overlap on different streams of one
+// device share the word.
+__device__ uint32_t g_mp_error;
 
 template <typename T>
 struct MP;
@@ -312,6 +318,77 @@ bool make_map(CUtensorMap* map, const T* ptr, int rows, int cols, int ld, int bo
 
 constexpr size_t kTmaSmem = (size_t)STAGES * (A_TILE + B_TILE) * 4 + STAGES * 8 + 1024;
 
+// Host-side state kept per device: the TMA kernels' dynamic shared-memory
+// attribute is a per-device setting, and the error word's device address is
+// looked up with that device current.
+constexpr int kMaxDevices = 64;
+struct DeviceState {
+  bool attr_f32 = false;
+  bool attr_i32 = false;
+  uint32_t* err = nullptr;
+};
+std::mutex g_dev_mu;
+DeviceState g_dev[kMaxDevices];
+
+cudaError_t current_state(DeviceState** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  *out = &g_dev[dev];
+  return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t ensure_smem_attr() {
+  DeviceState* d = nullptr;
+  cudaError_t e = current_state(&d);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_dev_mu);
+  bool& done = std::is_same<T, float>::value ? d->attr_f32 : d->attr_i32;
+  if (!done) {
+    e = cudaFuncSetAttribute(k_minplus_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmem);
+    if (e != cudaSuccess) return e;
+    done = true;
+  }
+  return cudaSuccess;
+}
+
+// Device address of g_mp_error on the current device.
+cudaError_t mp_error_ptr(uint32_t** out) {
+  DeviceState* d = nullptr;
+  cudaError_t e = current_state(&d);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_dev_mu);
+  if (!d->err) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_mp_error);
+    if (e != cudaSuccess) return e;
+    d->err = (uint32_t*)p;
+  }
+  *out = d->err;
+  return cudaSuccess;
+}
+
+// Stream-ordered clear of the error word (allocates nothing).
+cudaError_t clear_mp_error(cudaStream_t st) {
+  uint32_t* p = nullptr;
+  cudaError_t e = mp_error_ptr(&p);
+  if (e != cudaSuccess) return e;
+  return cudaMemsetAsync(p, 0, sizeof(uint32_t), st);
+}
+
+// Wait for the stream, then read the error word: B2_TIMEOUT when a wait of a
+// product issued since the last clear gave up.
+b2_status read_mp_error(cudaStream_t st) {
+  uint32_t* p = nullptr;
+  B2_CUDA_TRY(mp_error_ptr(&p));
+  uint32_t err = 0;
+  B2_CUDA_TRY(cudaMemcpyAsync(&err, p, sizeof(err), cudaMemcpyDeviceToHost, st));
+  B2_CUDA_TRY(cudaStreamSynchronize(st));
+  return err ? B2_TIMEOUT : B2_SUCCESS;
+}
+
 template <typename T>
 cudaError_t launch_minplus(const T* A, const T* B, T* C, int M, int N, int K, int lda, int ldb, int ldc,
                            cudaStream_t st, const T* Aold, uint32_t* changed) {
@@ -319,11 +396,8 @@ cudaError_t launch_minplus(const T* A, const T* B, T* C, int M, int N, int K, in
   CUtensorMap ma, mb;
   const bool tma = make_map<T>(&ma, A, M, K, lda, BK, BM, true) && make_map<T>(&mb, B, K, N, ldb, BN, BK, false);
   if (tma) {
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_minplus_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmem);
-      attr = true;
-    }
+    cudaError_t ea = ensure_smem_attr<T>();
+    if (ea != cudaSuccess) return ea;
     k_minplus_tma<T><<<tiles, NT, kTmaSmem, st>>>(ma, mb, C, M, N, K, ldc, Aold, lda, changed);
   } else {
     k_minplus_plain<T><<<tiles, NT, 0, st>>>(A, B, C, M, N, K, lda, ldb, ldc, Aold, changed);
@@ -335,6 +409,7 @@ template <typename T>
 b2_status gemm(const T* A, const T* B, T* C, int M, int N, int K, int lda, int ldb, int ldc, b2_stream s) {
   // argument rules of minplus_gemm_f32 (minplus_hip.cpp:132-142)
   if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0 || lda < K || ldb < N || ldc < N) return B2_INVALID_ARGUMENT;
+  B2_CUDA_TRY(clear_mp_error((cudaStream_t)s));
   return from_cuda(launch_minplus<T>(A, B, C, M, N, K, lda, ldb, ldc, (cudaStream_t)s, nullptr, nullptr));
 }
 
@@ -344,6 +419,7 @@ b2_status apsp(T* D, int N, b2_stream s, int32_t* squarings) {
   cudaStream_t st = (cudaStream_t)s;
   if (squarings) *squarings = 0;
   if (N == 1) return B2_SUCCESS;
+  B2_CUDA_TRY(clear_mp_error(st));
   T* tmp = nullptr;
   uint32_t* flag = nullptr;
   uint32_t* hflag = nullptr;
@@ -374,9 +450,7 @@ b2_status apsp(T* D, int N, b2_stream s, int32_t* squarings) {
   if (hflag) cudaFreeHost(hflag);
   if (squarings) *squarings = done;
   if (e != cudaSuccess) return from_cuda(e);
-  uint32_t err = 0;
-  cudaMemcpyFromSymbol(&err, g_mp_error, sizeof(err));
-  return err ? B2_TIMEOUT : B2_SUCCESS;
+  return read_mp_error(st);
 }
 
 // ---- ALU peak calibration (roofline denominator for min-plus) -------------
@@ -445,6 +519,10 @@ extern "C" b2_status b2_apsp_f32(float* d_D, int32_t N, b2_stream stream, int32_
 
 extern "C" b2_status b2_apsp_i32(int32_t* d_D, int32_t N, b2_stream stream, int32_t* sq) {
   return apsp<int>(d_D, N, stream, sq);
+}
+
+extern "C" b2_status b2_minplus_status(b2_stream stream) {
+  return read_mp_error((cudaStream_t)stream);
 }
 
 extern "C" b2_status b2_minplus_calibrate(int32_t is_float, double* pairs_per_second) {
@@ -540,6 +618,7 @@ extern "C" b2_status b2_apsp_f32_noalloc(float* d_D, int32_t N, b2_stream stream
   if (N == 1) return B2_SUCCESS;
   unsigned char* base = nullptr;
   B2_CUDA_TRY(noalloc_scratch(&base));
+  B2_CUDA_TRY(clear_mp_error(st));
   float* tmp = (float*)base;
   uint32_t* flag = (uint32_t*)(base + kNoAllocScratchBytes);
   int maxsq = 0;
@@ -565,7 +644,5 @@ extern "C" b2_status b2_apsp_f32_noalloc(float* d_D, int32_t N, b2_stream stream
   }
   if (squarings) *squarings = done;
   if (e != cudaSuccess) return from_cuda(e);
-  uint32_t err = 0;
-  cudaMemcpyFromSymbol(&err, g_mp_error, sizeof(err));
-  return err ? B2_TIMEOUT : B2_SUCCESS;
+  return read_mp_error(st);
 }

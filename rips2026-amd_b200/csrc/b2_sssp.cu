@@ -1407,18 +1407,26 @@ __global__ void k_reach(uint32_t n, const uint64_t* rowptr, const void* labels, 
 
 // ---------------------------------------------------------------------------
 // host side
+// Co-resident grid of one kernel instance on the current device.  The
+// shared-memory attribute and the occupancy are per-device facts, so both are
+// settled once per (instance, device).
+constexpr int kMaxDevices = 64;
 template <class W, bool PRED, int MODE>
 int max_grid() {
-  static int cached = 0;
-  if (cached) return cached;
+  static std::mutex mu;
+  static int cached[kMaxDevices] = {};
   int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (cached[dev]) return cached[dev];
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaFuncSetAttribute(k_sssp<W, PRED, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+  if (cudaFuncSetAttribute(k_sssp<W, PRED, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes) !=
+      cudaSuccess)
+    return 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sssp<W, PRED, MODE>, kThreads, kStageBytes);
   if (per < 1) per = 1;
-  cached = per * sms;
-  return cached;
+  cached[dev] = per * sms;
+  return cached[dev];
 }
 
 template <class W, bool PRED, int MODE>
@@ -1627,7 +1635,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   do {                                                                     \
     grid = max_grid<WT, PR, MD>();                                         \
     if (o.grid_blocks && (int)o.grid_blocks < grid) grid = o.grid_blocks;  \
-    e = launch<WT, PR, MD>(P, grid, st);                                   \
+    e = grid > 0 ? launch<WT, PR, MD>(P, grid, st) : cudaErrorInvalidConfiguration; \
   } while (0)
   if (mode == kModeBF) {
     if (isf) { if (pred) B2_LAUNCH(WF32, true, kModeBF); else B2_LAUNCH(WF32, false, kModeBF); }

@@ -280,7 +280,9 @@ def tiny_fixtures(ref: str) -> None:
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if a != "--only" and a != "tiny"]
-    ref_dir = args[0] if args else "/root/reference"
+    ref_dir = args[0] if args else os.environ.get("B2_REFERENCE_DIR", "")
+    if not ref_dir or not os.path.isdir(ref_dir):
+        sys.exit("usage: make_golden.py <reference checkout> [--only tiny]  (or set B2_REFERENCE_DIR)")
     if "--only" in sys.argv:
         tiny_fixtures(ref_dir)
     else:

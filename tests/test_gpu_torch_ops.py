@@ -43,3 +43,27 @@ def test_min_plus_matmul_op_matches_oracle(ops, orc, cuda):
     A[rng.random(A.shape) < 0.5] = np.inf
     C = ops.min_plus_matmul(cuda.from_numpy(A).cuda(), cuda.from_numpy(B).cuda())
     assert np.array_equal(C.cpu().numpy(), orc.minplus_gemm(A, B))
+
+
+def test_bellman_ford_op_int32_weights(ops, b2, orc, cuda):
+    """int32 weights are solved exactly (int32 distances); a negative int32
+    weight is refused, and the same negative weights as float32 go through the
+    reference's negative-weight rules, negative-cycle flag included."""
+    hg = b2.gen_er(1500, 12000, 1, 100, seed=74)
+    inc = hg.transpose()
+    t = lambda a: cuda.from_numpy(np.ascontiguousarray(a)).cuda()
+    wi = inc.weights.view(np.int32)
+    dist, pred, iters, conv, negc = ops.sssp_min_plus_bellman_ford(t(inc.rowptr), t(inc.colind), t(wi), 3)
+    assert dist.dtype == cuda.int32
+    assert np.array_equal(dist.cpu().numpy().view(np.uint32), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 3))
+    assert conv and not negc
+    bad = wi.copy()
+    bad[5] = -3
+    with pytest.raises(ValueError, match="negative int32"):
+        ops.sssp_min_plus_bellman_ford(t(inc.rowptr), t(inc.colind), t(bad), 3)
+    # incoming CSR of 0->1 (1), 2->1 (1), 1->2 (-2): the cycle 1->2->1 weighs -1
+    rp = np.array([0, 0, 2, 3], np.int64)
+    ci = np.array([0, 2, 1], np.int32)
+    wf = np.array([1.0, 1.0, -2.0], np.float32)
+    dist, pred, iters, conv, negc = ops.sssp_min_plus_bellman_ford(t(rp), t(ci), t(wf), 0)
+    assert dist.dtype == cuda.float32 and negc and not conv

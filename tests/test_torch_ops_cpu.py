@@ -30,3 +30,16 @@ def test_cpu_tensors_are_refused(ops):
         ops.bucketted_bellman_ford(rp, ci, w, 0, 2)
     with pytest.raises(ValueError, match="CUDA"):
         ops.min_plus_matmul(torch.zeros(2, 2), torch.zeros(2, 2))
+
+
+def test_fake_kernels_follow_the_value_dtype(ops):
+    """Under FakeTensorMode (torch.compile tracing) the distance dtype is the
+    real op's: float32 for float32 weights, int32 for int32 weights."""
+    from torch._subclasses.fake_tensor import FakeTensorMode
+    with FakeTensorMode():
+        rp = torch.empty(5, dtype=torch.int64)
+        ci = torch.empty(4, dtype=torch.int32)
+        for vdt, ddt in ((torch.float32, torch.float32), (torch.int32, torch.int32)):
+            d, p, *_ = ops.sssp_min_plus_bellman_ford(rp, ci, torch.empty(4, dtype=vdt), 0)
+            assert d.dtype == ddt and d.shape == (4,)
+            assert p.dtype == torch.int64

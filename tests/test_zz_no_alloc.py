@@ -27,9 +27,12 @@ def test_noalloc_apsp_matches_allocating_entry_point(b2, cuda):
     from b200sssp import _lib
     L = _lib.lib()
     rng = np.random.default_rng(2026)
-    for n in (700, 301):          # two calls in a row, the second smaller than the first
+    # two calls in a row, the second smaller than the first, then the exact fit
+    # (a 2048 x 2048 matrix fills the scratch up to the change flag) and the
+    # one-vertex case (nothing to square)
+    for n in (700, 301, 2048, 1):
         D = rng.uniform(0, 1, (n, n)).astype(np.float32)
-        D[rng.uniform(size=D.shape) < 0.97] = np.inf
+        D[rng.uniform(size=D.shape) < (0.97 if n < 1000 else 0.995)] = np.inf
         np.fill_diagonal(D, 0)
         a = torch.from_numpy(D).cuda()
         b = a.clone()
