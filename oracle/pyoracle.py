@@ -24,16 +24,16 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
-SRC = os.path.join(HERE, "oracle.c")
+SRCS = [os.path.join(HERE, "oracle.c"), os.path.join(HERE, "oracle_gen.c")]
 
 _lib = None
 
 
 def build_oracle(force: bool = False) -> str:
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in SRCS):
         tmp = LIB + ".tmp"
-        subprocess.run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-o", tmp, SRC,
-                        "-lm"], check=True)
+        subprocess.run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-pthread", "-o", tmp,
+                        *SRCS, "-lm"], check=True)
         os.replace(tmp, LIB)
     return LIB
 
@@ -59,8 +59,71 @@ def lib() -> C.CDLL:
             getattr(L, nm).restype = i64
         L.orc_validate_spt.argtypes = [i64, P, P, P, C.c_int, i64, P, P]
         L.orc_validate_spt.restype = C.c_int
+        pp = C.POINTER(C.c_void_p)
+        L.orc_gen_rmat.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint32,
+                                   C.c_uint64, C.c_int, C.POINTER(i64), C.POINTER(i64), pp, pp, pp]
+        L.orc_gen_grid.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int,
+                                   C.POINTER(i64), C.POINTER(i64), pp, pp, pp, C.POINTER(C.c_uint32)]
+        L.orc_free.argtypes = [P]
         _lib = L
     return _lib
+
+
+def _host_threads() -> int:
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def _take(ptr: C.c_void_p, count: int, dtype) -> np.ndarray:
+    """Copy a malloc'd C array into numpy and free it."""
+    L = lib()
+    try:
+        if count == 0:
+            return np.zeros(0, dtype)
+        buf = (C.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr.value)
+        return np.frombuffer(buf, dtype=dtype, count=count).copy()
+    finally:
+        L.orc_free(ptr)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             wmin: int = 1, wmax: int = 255, seed: int = 0, threads: int | None = None):
+    """Twin of the library's RMAT generator (oracle_gen.c): OUTGOING CSR
+    (rowptr int64, colind int32, weights uint32, fweights float32), the same
+    bytes as b2_gen_rmat for the same arguments."""
+    L = lib()
+    n, m = C.c_int64(), C.c_int64()
+    rp, ci, w = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    r = L.orc_gen_rmat(scale, edge_factor, a, b, c, wmin, wmax, seed, threads or _host_threads(), C.byref(n),
+                       C.byref(m), C.byref(rp), C.byref(ci), C.byref(w))
+    if r != 0:
+        raise ValueError(f"orc_gen_rmat failed ({r})")
+    rowptr = _take(rp, n.value + 1, np.int64)
+    colind = _take(ci, m.value, np.int32)
+    weights = _take(w, m.value, np.uint32)
+    fweights = weights.astype(np.float32) / np.float32(float(wmax) + 1.0)
+    return rowptr, colind, weights, fweights
+
+
+def gen_grid(rows: int, cols: int, shortcut_frac: float = 0.02, mu: float = 5.0, sigma: float = 1.0,
+             seed: int = 0, threads: int | None = None):
+    """Twin of the library's road-like grid generator (oracle_gen.c): the same
+    bytes as b2_gen_grid (float weights w / (max w + 1))."""
+    L = lib()
+    n, m = C.c_int64(), C.c_int64()
+    rp, ci, w = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    mx = C.c_uint32()
+    r = L.orc_gen_grid(rows, cols, shortcut_frac, mu, sigma, seed, threads or _host_threads(), C.byref(n),
+                       C.byref(m), C.byref(rp), C.byref(ci), C.byref(w), C.byref(mx))
+    if r != 0:
+        raise ValueError(f"orc_gen_grid failed ({r})")
+    rowptr = _take(rp, n.value + 1, np.int64)
+    colind = _take(ci, m.value, np.int32)
+    weights = _take(w, m.value, np.uint32)
+    fweights = weights.astype(np.float32) / np.float32(float(mx.value) + 1.0)
+    return rowptr, colind, weights, fweights
 
 
 def _p(a: np.ndarray) -> int:
@@ -198,6 +261,68 @@ def sssp_min_plus_bellman_ford(indptr, indices, data, source: int, max_iters: in
             break
         d = d_new
     d_check = np.minimum(d, tropical_spmv(indptr, indices, data, d))
+    neg = not np.all(np.isclose(d_check, d) | (np.isinf(d_check) & np.isinf(d)))
+    return d, used, converged, neg
+
+
+class RowBlocks:
+    """An INCOMING CSR cut into row blocks of about equal arc counts, one per
+    host thread, for the row-parallel form of sssp_min_plus_bellman_ford."""
+
+    def __init__(self, indptr, indices, data, threads: int | None = None):
+        indptr = np.asarray(indptr, np.int64)
+        self.n = indptr.shape[0] - 1
+        self.m = int(indptr[-1])
+        self.threads = max(1, threads or _host_threads())
+        cuts = np.searchsorted(indptr, np.linspace(0, self.m, self.threads + 1)).tolist()
+        cuts[0], cuts[-1] = 0, self.n
+        self.blocks = []
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            if b <= a:
+                continue
+            e0, e1 = int(indptr[a]), int(indptr[b])
+            self.blocks.append((a, b, indptr[a:b + 1] - e0, np.asarray(indices[e0:e1]),
+                                np.asarray(data[e0:e1], np.float64)))
+        from concurrent.futures import ThreadPoolExecutor
+        self.pool = ThreadPoolExecutor(max_workers=len(self.blocks) or 1)
+
+    def relax(self, d: np.ndarray) -> np.ndarray:
+        """np.minimum(d, tropical_spmv(A, d)), block by block (numpy's gather
+        and reduceat release the GIL, so the blocks run in parallel)."""
+        out = np.empty_like(d)
+
+        def one(blk):
+            a, b, rp, ci, dv = blk
+            out[a:b] = np.minimum(d[a:b], tropical_spmv(rp, ci, dv, d))
+
+        list(self.pool.map(one, self.blocks))
+        return out
+
+    def close(self):
+        self.pool.shutdown()
+
+
+def sssp_min_plus_bellman_ford_rows(A: RowBlocks, source: int, max_iters: int | None = None):
+    """sssp_min_plus_bellman_ford (minplus_bellman_ford.py:51-102, track_pred=False)
+    with every round's tropical SpMV split into row blocks over host threads:
+    the same rounds, the same stopping test and the same negative-cycle round,
+    so the same (dist, iterations_used, converged, has_negative_cycle)."""
+    n = A.n
+    if max_iters is None:
+        max_iters = n - 1
+    d = np.full(n, INF)
+    d[source] = 0.0
+    converged = False
+    used = 0
+    for it in range(max_iters):
+        used = it + 1
+        d_new = A.relax(d)
+        if np.array_equal(d_new, d) or np.all(np.isclose(d_new, d) | (np.isinf(d_new) & np.isinf(d))):
+            d = d_new
+            converged = True
+            break
+        d = d_new
+    d_check = A.relax(d)
     neg = not np.all(np.isclose(d_check, d) | (np.isinf(d_check) & np.isinf(d)))
     return d, used, converged, neg
 

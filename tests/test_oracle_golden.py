@@ -180,3 +180,23 @@ def test_spt_validator_detects_errors(orc, b2):
     v = int(np.nonzero(bad >= 0)[0][0])
     bad[v] = (bad[v] + 1) % g.n
     assert orc.validate_spt(g.rowptr, g.colind, g.weights, 0, d, bad) != 0
+
+
+def test_row_parallel_reference_bf_equals_the_serial_port(orc):
+    """The row-block form of the reference's Bellman-Ford (bench.py's reference
+    arm) gives the serial port's result word for word, rounds and flags too."""
+    rng = np.random.default_rng(5)
+    for n, m, neg in ((3000, 24000, False), (500, 3000, True)):
+        src = rng.integers(0, n, m)
+        dst = rng.integers(0, n, m)
+        w = rng.uniform(-0.2 if neg else 0.0, 1.0, m)
+        order = np.lexsort((src, dst))
+        src, dst, w = src[order], dst[order], w[order]
+        rp = np.zeros(n + 1, np.int64)
+        np.add.at(rp, dst + 1, 1)
+        rp = np.cumsum(rp)
+        want = orc.sssp_min_plus_bellman_ford(rp, src.astype(np.int32), w, 0)
+        A = orc.RowBlocks(rp, src.astype(np.int32), w, threads=4)
+        got = orc.sssp_min_plus_bellman_ford_rows(A, 0)
+        A.close()
+        assert np.array_equal(got[0], want[0]) and got[1:] == want[1:]
