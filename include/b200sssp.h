@@ -132,7 +132,10 @@ typedef struct b2_sssp_opts {
                                heavy out-edges (default 8); the incoming CSR is built on first
                                use, only for graphs with m >= pull_fraction x n; <= 0: push only */
   uint32_t grid_blocks;     /* 0: occupancy-derived persistent grid */
-  double timeout_ms;        /* bound on every device wait (default 20000) */
+  double timeout_ms;        /* bound on the whole solve and on every device wait, in ms
+                               (default 20000; fractions of a millisecond allowed): past it the
+                               kernel stops at its next wait or phase boundary and the call
+                               returns B2_TIMEOUT; the graph handle stays usable */
   int32_t collect_reach;    /* fill stats.reached / reached_edges (one extra O(n) pass) */
   int32_t detect_negative_cycle; /* BF: one extra round after max_iters (python reference rule) */
   int32_t light_heavy;      /* delta: relax light edges (w <= delta) per sub-phase and heavy
@@ -144,6 +147,25 @@ typedef struct b2_sssp_opts {
                                queue (ordered access to labels and rows); 0 (default): 1/16
                                on graphs whose largest out-degree is <= 64, else the queue;
                                < 0: always the queue */
+  uint32_t worklist_capacity; /* delta / ADDS / BF: entries each device worklist may hold; 0
+                               (default): n, which no solve can exceed.  A smaller value bounds
+                               the queues like the reference's fixed-capacity frontier queues
+                               (delta_stepping_hip_CSR.cpp:616-620): a solve that would push
+                               past it stops and returns B2_POOL_EXHAUSTED */
+  int32_t keep_distances;   /* ADDS only: 1 = warm start -- d_dist holds starting distances
+                               (input ids; uint32 0xFFFFFFFF or float +inf = none) that stay
+                               as upper bounds; only the source (set to 0) starts queued, so
+                               only vertices a path from the source improves are expanded.
+                               hip_adds::Options::initialize_distances = false
+                               (hip_adds_sssp.hpp:64-66).  0 (default): every distance starts
+                               at infinity.  Other methods return B2_NOT_SUPPORTED for 1. */
+  uint32_t active_buckets;  /* ADDS: buckets from the lowest unfinished one that warps may take
+                               entries from at the start of a window (0: 2); grows while warps
+                               idle and later buckets hold work (the reference's dynamic
+                               active-bucket count, hip_adds_sssp.hpp:37-38) */
+  int32_t adds_fixed_delta; /* ADDS: 1 keeps the bucket width fixed (the reference's
+                               dynamic_delta = false); 0 (default): growth 1.5 / shrink 0.75 at
+                               every new window from the last window's utilization */
   int32_t reserved[3];
 } b2_sssp_opts;
 
@@ -177,6 +199,9 @@ typedef struct b2_stats {
   double delta_final;       /* ADDS: bucket width at the end (delta: = delta_used) */
   uint32_t policy_used;     /* 1: the learned policy chose delta / fusion / light-heavy */
   uint32_t heavy_pulls;     /* heavy passes run in the pull direction */
+  uint64_t work_items;      /* ADDS: bucket-queue entries and hub chunks taken by warps */
+  uint32_t active_buckets_max; /* ADDS: widest range of buckets warps took entries from */
+  uint32_t reserved0;
 } b2_stats;
 
 /* ---- library ---------------------------------------------------------- */

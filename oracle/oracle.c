@@ -80,11 +80,18 @@ static hitem hpop(heap* h) {
   return top;
 }
 
-/* uint32 weights, saturating sums; INF = 0xFFFFFFFF. */
-void orc_dijkstra_u32(int64_t n, const int64_t* rp, const int32_t* ci, const uint32_t* w, int64_t src,
-                      uint32_t* dist) {
+/* uint32 weights, saturating sums; INF = 0xFFFFFFFF.
+ * keep_labels = 0: every label starts at INF.  keep_labels = 1: the labels
+ * already in `dist` are kept as upper bounds and only the source (set to 0)
+ * starts in the queue, so only vertices that a path from the source improves
+ * are ever expanded -- the warm start of hip_adds::sssp with
+ * Options::initialize_distances = false (hip_adds_sssp.hpp:64-66, its
+ * init_kernel hip_adds_sssp.cpp:873-908). */
+void orc_dijkstra_u32_from(int64_t n, const int64_t* rp, const int32_t* ci, const uint32_t* w, int64_t src,
+                           uint32_t* dist, int keep_labels) {
   heap h = {0, 0, 0, 1};
-  for (int64_t i = 0; i < n; ++i) dist[i] = 0xFFFFFFFFu;
+  if (!keep_labels)
+    for (int64_t i = 0; i < n; ++i) dist[i] = 0xFFFFFFFFu;
   dist[src] = 0;
   hitem s0 = {0.0, 0, (uint32_t)src};
   hpush(&h, s0);
@@ -104,6 +111,11 @@ void orc_dijkstra_u32(int64_t n, const int64_t* rp, const int32_t* ci, const uin
     }
   }
   free(h.a);
+}
+
+void orc_dijkstra_u32(int64_t n, const int64_t* rp, const int32_t* ci, const uint32_t* w, int64_t src,
+                      uint32_t* dist) {
+  orc_dijkstra_u32_from(n, rp, ci, w, src, dist, 0);
 }
 
 /* uint32 Dijkstra ordered by (dist, hops): hops[v] = fewest arcs among the
@@ -143,11 +155,13 @@ int64_t orc_dijkstra_u32_hops(int64_t n, const int64_t* rp, const int32_t* ci, c
   return mx;
 }
 
-/* float weights >= 0, float accumulation; unreachable = +inf. */
-void orc_dijkstra_f32(int64_t n, const int64_t* rp, const int32_t* ci, const float* w, int64_t src,
-                      float* dist) {
+/* float weights >= 0, float accumulation; unreachable = +inf.  keep_labels as
+ * for orc_dijkstra_u32_from. */
+void orc_dijkstra_f32_from(int64_t n, const int64_t* rp, const int32_t* ci, const float* w, int64_t src,
+                           float* dist, int keep_labels) {
   heap h = {0, 0, 0, 0};
-  for (int64_t i = 0; i < n; ++i) dist[i] = INFINITY;
+  if (!keep_labels)
+    for (int64_t i = 0; i < n; ++i) dist[i] = INFINITY;
   dist[src] = 0.0f;
   hitem s0 = {0.0, 0, (uint32_t)src};
   hpush(&h, s0);
@@ -166,6 +180,11 @@ void orc_dijkstra_f32(int64_t n, const int64_t* rp, const int32_t* ci, const flo
     }
   }
   free(h.a);
+}
+
+void orc_dijkstra_f32(int64_t n, const int64_t* rp, const int32_t* ci, const float* w, int64_t src,
+                      float* dist) {
+  orc_dijkstra_f32_from(n, rp, ci, w, src, dist, 0);
 }
 
 void orc_dijkstra_f64(int64_t n, const int64_t* rp, const int32_t* ci, const double* w, int64_t src,

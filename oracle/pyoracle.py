@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
         L.orc_dijkstra_u32_hops.argtypes = [i64, P, P, P, i64, P, P]
         L.orc_dijkstra_u32_hops.restype = i64
         L.orc_dijkstra_f64.argtypes = [i64, P, P, P, i64, P]
+        L.orc_dijkstra_u32_from.argtypes = [i64, P, P, P, i64, P, C.c_int]
+        L.orc_dijkstra_f32_from.argtypes = [i64, P, P, P, i64, P, C.c_int]
         L.orc_bf_jacobi_f32.argtypes = [i64, P, P, P, i64, i64, C.c_int, P, P]
         L.orc_bf_jacobi_f64.argtypes = [i64, P, P, P, i64, i64, C.c_int, P, P]
         L.orc_minplus_gemm_f32.argtypes = [P, P, P, i64, i64, i64, i64, i64, i64]
@@ -151,6 +153,22 @@ def dijkstra(rowptr, colind, weights, source: int) -> np.ndarray:
         d = np.empty(n, np.float64)
         lib().orc_dijkstra_f64(n, _p(rp), _p(ci), _p(w), source, _p(d))
     return d
+
+
+def dijkstra_warm(rowptr, colind, weights, source: int, initial: np.ndarray) -> np.ndarray:
+    """Dijkstra that keeps `initial` as upper bounds and starts from the source
+    alone (hip_adds::sssp with initialize_distances = false): uint32 or float32."""
+    rp, ci = _csr(rowptr, colind)
+    n = rp.shape[0] - 1
+    w = np.ascontiguousarray(weights)
+    if w.dtype == np.uint32:
+        out = np.array(initial, dtype=np.uint32, copy=True)
+        lib().orc_dijkstra_u32_from(n, _p(rp), _p(ci), _p(w), source, _p(out), 1)
+    else:
+        w = np.ascontiguousarray(w, np.float32)
+        out = np.array(initial, dtype=np.float32, copy=True)
+        lib().orc_dijkstra_f32_from(n, _p(rp), _p(ci), _p(w), source, _p(out), 1)
+    return out
 
 
 def bf_iterations_u32(rowptr, colind, weights, source: int) -> tuple[int, np.ndarray]:

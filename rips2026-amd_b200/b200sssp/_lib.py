@@ -52,7 +52,8 @@ class Opts(C.Structure):
                 ("pull_fraction", C.c_float), ("grid_blocks", C.c_uint32),
                 ("timeout_ms", C.c_double), ("collect_reach", C.c_int32),
                 ("detect_negative_cycle", C.c_int32), ("light_heavy", C.c_int32), ("trace", C.c_int32),
-                ("dense_fraction", C.c_float), ("reserved", C.c_int32 * 3)]
+                ("dense_fraction", C.c_float), ("worklist_capacity", C.c_uint32), ("keep_distances", C.c_int32),
+                ("active_buckets", C.c_uint32), ("adds_fixed_delta", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class TraceEntry(C.Structure):
@@ -68,7 +69,8 @@ class Stats(C.Structure):
                 ("delta_used", C.c_double), ("kernel_ms", C.c_float), ("device_error", C.c_uint32),
                 ("grid_blocks", C.c_uint32), ("first_unchanged", C.c_uint32),
                 ("local_subphases", C.c_uint32), ("delta_updates", C.c_uint32),
-                ("delta_final", C.c_double), ("policy_used", C.c_uint32), ("heavy_pulls", C.c_uint32)]
+                ("delta_final", C.c_double), ("policy_used", C.c_uint32), ("heavy_pulls", C.c_uint32),
+                ("work_items", C.c_uint64), ("active_buckets_max", C.c_uint32), ("reserved0", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

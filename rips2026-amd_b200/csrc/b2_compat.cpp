@@ -628,7 +628,6 @@ Status run(const DeviceCsrGraph<Weight>& graph, uint32_t source, Weight* d_dista
            const Options& options, cudaStream_t stream, int wt) {
   if (graph.num_vertices == 0 || source >= graph.num_vertices || d_distances == nullptr) return Status::InvalidArgument;
   if (!graph.row_offsets || (graph.num_edges && (!graph.col_indices || !graph.weights))) return Status::InvalidArgument;
-  if (!options.initialize_distances) return Status::InvalidArgument;   // warm starts are not supported
   b2_csr csr = {graph.num_vertices, graph.num_vertices, graph.num_edges, graph.row_offsets,
                 reinterpret_cast<const int32_t*>(graph.col_indices), graph.weights, 32, wt, B2_OUTGOING, 1};
   b2_graph g = nullptr;
@@ -638,20 +637,27 @@ Status run(const DeviceCsrGraph<Weight>& graph, uint32_t source, Weight* d_dista
   b2_sssp_opts_default(&o);
   if (options.initial_delta > 0.0) o.delta = options.initial_delta;
   o.delta_scale = options.initial_delta_scale;
+  o.keep_distances = options.initialize_distances ? 0 : 1;   // warm start (hip_adds_sssp.hpp:64-66)
+  o.adds_fixed_delta = options.dynamic_delta ? 0 : 1;
+  o.active_buckets = options.initial_active_buckets;
+  if (options.worker_blocks) o.grid_blocks = options.worker_blocks;
+  // pool_words is the reference's whole worklist pool; here each of the
+  // window queues and far piles holds an equal share
+  if (options.pool_words) o.worklist_capacity = (uint32_t)std::min<size_t>(std::max<size_t>(options.pool_words / 34, 1),
+                                                                            0xFFFFFFFFull);
   b2_stats st;
-  s = options.dynamic_delta ? b2_sssp_adds(g, source, d_distances, nullptr, &o, stream, &st)
-                            : b2_sssp_delta(g, source, d_distances, nullptr, &o, stream, &st);
+  s = b2_sssp_adds(g, source, d_distances, nullptr, &o, stream, &st);
   b2_graph_destroy(g);
   if (stats) {
     *stats = RunStats();
     stats->initial_delta = st.delta_used;
     stats->final_delta = st.delta_final;
     stats->worker_blocks = st.grid_blocks;
-    stats->final_active_buckets = 1;
+    stats->final_active_buckets = st.active_buckets_max;
     stats->device_error = st.device_error;
-    stats->assigned_items = st.pushes;
-    stats->processed_items = st.pushes;
-    stats->enqueued_items = st.pushes;
+    stats->assigned_items = st.work_items;
+    stats->processed_items = st.work_items;
+    stats->enqueued_items = st.pushes + 1;   // + the source
     stats->edge_relaxations = st.edges_scanned;
     stats->successful_relaxations = st.improvements;
     stats->head_switches = (uint64_t)st.iterations_used;

@@ -435,6 +435,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   fr(w.hstamp); fr(w.lightcnt); fr(w.in_lightcnt); fr(w.trace);
   fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
+  free_adds_workspace(w);
   w = Workspace();
   const size_t word = pred ? 8 : 4;
   w.n = n;
@@ -588,6 +589,7 @@ extern "C" b2_status b2_graph_destroy(b2_graph g) {
   fr(w.hstamp); fr(w.lightcnt); fr(w.in_lightcnt); fr(w.trace);
   fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
+  free_adds_workspace(w);
   delete g;
   return B2_SUCCESS;
 }

@@ -156,6 +156,66 @@ struct Control {
   unsigned long long pushes;
 };
 
+// ---- asynchronous ADDS worklist (b2_adds.cu) ------------------------------
+// Buckets of one window epoch: slot s holds global bucket W + s.  Each slot is
+// an append-only queue with its own counters on a 128-byte line.
+constexpr int kAddsSlots = 32;
+struct alignas(128) AddsSlot {
+  unsigned long long claim;   // (epoch << 32) | entries claimed by warps
+  uint32_t reserved;          // entries reserved by writers
+  uint32_t extra;             // hub chunks spawned by this bucket's entries
+  uint32_t done;              // entries and hub chunks finished
+  uint32_t pad[27];
+};
+static_assert(sizeof(AddsSlot) == 128, "slot line");
+
+struct alignas(128) AddsControl {
+  // grid barrier (start of the solve only); must stay first
+  uint32_t bar_arrive;
+  uint32_t bar_gen;
+  uint32_t error;
+  uint32_t error_site;
+  uint32_t pad0[28];
+  AddsSlot slot[kAddsSlots];
+  // window epoch: written by the one warp that prepares a split while every
+  // other warp waits; `epoch` is written last
+  uint32_t state;             // AddsState
+  uint32_t epoch;
+  uint32_t head;              // first bucket of the epoch not yet retired (0..kAddsSlots)
+  uint32_t W;                 // global number of slot 0's bucket
+  uint32_t kbase;             // distance key at which slot 0 starts
+  uint32_t dq;                // bucket width (uint32 graphs)
+  uint32_t dinv;              // float bits of 1 / width (float graphs)
+  uint32_t far_sel;           // far pile receiving pushes past the window
+  uint32_t far_count[2];
+  uint32_t far_min_key;       // smallest key pushed into the far pile this epoch
+  uint32_t active;            // buckets from head on that warps may take entries from
+  uint32_t pad1[20];
+  unsigned long long hub_claim;   // hub chunks claimed
+  unsigned long long hub_reserved;
+  uint32_t pad2[28];
+  uint32_t split_cursor;
+  uint32_t split_done;
+  uint32_t split_total;
+  uint32_t trace_n;
+  // statistics
+  unsigned long long edges;
+  unsigned long long improvements;
+  unsigned long long pushes;
+  unsigned long long entries;     // entries taken from bucket queues
+  unsigned long long hub_chunks;
+  unsigned long long t_start;
+  uint32_t buckets;               // non-empty buckets retired
+  uint32_t epochs;
+  uint32_t delta_updates;
+  uint32_t max_active;
+  unsigned long long epoch_entries;
+  uint32_t epoch_buckets;
+  uint32_t converged;
+};
+
+enum AddsState : uint32_t { kAddsRun = 0, kAddsSplitPrep = 1, kAddsSplit = 2, kAddsDone = 3 };
+
 // Per-graph solver workspace, sized for n vertices (allocated on first use).
 struct Workspace {
   size_t n = 0;
@@ -182,6 +242,15 @@ struct Workspace {
   unsigned long long* reach = nullptr;   // [reached vertices, their out-edges] of the last solve
   uint32_t phase_epoch = 0;
   size_t bytes = 0;
+  // ADDS worklist (allocated on the first b2_sssp_adds solve)
+  uint32_t* adds_q = nullptr;       // (kAddsSlots + 2) queues of adds_cap entries: window slots, 2 far piles
+  size_t adds_cap = 0;
+  uint2* adds_hub = nullptr;        // ring of hub chunks {v, chunk << 5 | slot}
+  size_t adds_hub_cap = 0;
+  uint32_t* adds_qb = nullptr;      // per vertex: global bucket it is queued in (unprocessed), else ~0
+  AddsControl* adds_ctl = nullptr;
+  AddsControl* adds_h_ctl = nullptr;
+  bool adds_dirty = true;           // queue entries must be reset to empty before the next solve
 };
 
 }  // namespace b2
@@ -219,6 +288,12 @@ struct b2_graph_s {
 
 namespace b2 {
 b2_status ensure_workspace(b2_graph g, bool pred);
+void free_adds_workspace(Workspace& w);
+// Asynchronous ADDS worklist solve (b2_adds.cu).
+b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, const b2_sssp_opts* o,
+                   cudaStream_t st, b2_stats* stats);
+// stats->reached / reached_edges from a solve's labels (keys, or key|pred words when pred).
+b2_status collect_reach(b2_graph g, const void* labels, bool pred, bool isf, cudaStream_t st, b2_stats* stats);
 b2_status ensure_incoming(b2_graph g, cudaStream_t st);
 // Internal id of input vertex `v` (identity unless the graph is in degree order).
 inline uint32_t internal_id(b2_graph g, uint32_t v) { return g->inv_host.empty() ? v : g->inv_host[v]; }

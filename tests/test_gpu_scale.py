@@ -1,0 +1,113 @@
+"""GPU parity at the benchmarked scales, and the fault paths a solve can take.
+
+* dense min-plus at N = 8192 (the C2d size), int32 and fp32: 64 sampled rows
+  of C = A (min,+) A against the oracle's GEMM on those rows, word for word;
+* min-plus SpGEMM on ER 2^20 with average degree 8 (the C2s size): the whole
+  product against the oracle's C SpGEMM, word for word (sorted columns);
+* FP32-weight RMAT and grid graphs of 2^20 vertices: delta-stepping and ADDS
+  against a float32 Dijkstra, word for word, predecessors as shortest-path
+  trees;
+* a solve whose budget runs out returns B2_TIMEOUT and the next solve on the
+  same handle is exact; a worklist bounded below what the solve needs returns
+  B2_POOL_EXHAUSTED (the reference's queue-overflow error) and the next solve
+  is exact.  Both are bounded waits that end on the device: nothing faults.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _u32(t):
+    return t.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("dtype", ["int32", "fp32"])
+def test_minplus_n8192_sampled_rows(b2, orc, cuda, dtype):
+    torch = cuda
+    from b200sssp import minplus
+    N = 8192
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    pres = torch.rand(N, N, device="cuda", generator=g) < 0.3
+    if dtype == "int32":
+        A = torch.randint(1, 1001, (N, N), device="cuda", generator=g, dtype=torch.int32)
+        A[~pres] = minplus.MISSING_I32
+    else:
+        A = torch.rand(N, N, device="cuda", generator=g)
+        A[~pres] = float("inf")
+    A.fill_diagonal_(0)
+    del pres
+    C = minplus.minplus_gemm(A, A)
+    rows = np.random.default_rng(4).choice(N, size=64, replace=False)
+    Ah = A.cpu().numpy()
+    ref = orc.minplus_gemm(np.ascontiguousarray(Ah[rows]), Ah)
+    got = C.cpu().numpy()[rows]
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("dtype", ["int32", "fp32"])
+def test_spgemm_er20_whole_product(b2, orc, cuda, dtype):
+    torch = cuda
+    from b200sssp import minplus
+    n = 1 << 20
+    hg = b2.gen_er(n, 8 * n, 1, 1000, 11)
+    vals = hg.weights.view(np.int32) if dtype == "int32" else hg.weights.astype(np.float32) / np.float32(1001.0)
+    A = (torch.from_numpy(hg.rowptr).cuda(), torch.from_numpy(hg.colind).cuda(), torch.from_numpy(vals).cuda(), n)
+    crp, cci, cv = (x.cpu().numpy() for x in minplus.minplus_spgemm(A, A))
+    host = (hg.rowptr, hg.colind, vals)
+    rrp, rci, rv = orc.minplus_spgemm(host, host, n)
+    assert np.array_equal(crp, rrp)
+    # oracle rows are unsorted: sort each row's (column, value) by column
+    row = np.repeat(np.arange(n), np.diff(rrp))
+    o = np.lexsort((rci, row))
+    assert np.array_equal(cci, rci[o])
+    assert np.array_equal(cv.view(np.uint32), rv[o].view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", ["rmat20", "grid1024"])
+@pytest.mark.parametrize("method", ["delta", "adds"])
+def test_f32_large_graphs_exact(b2, orc, cuda, kind, method):
+    hg = (b2.gen_rmat(20, 16, 0.57, 0.19, 0.19, 1, 255, 5) if kind == "rmat20"
+          else b2.gen_grid(1024, 1024, 0.02, 5.0, 1.0, 5))
+    g = b2.Graph.from_host(hg, "f32")
+    deg = np.diff(hg.rowptr)
+    srcs = [int(s) for s in np.flatnonzero(deg)[[0, 777, 4321]]]
+    for s in srcs:
+        d, p, st = g.sssp(s, method=method, pred=True)
+        got = d.cpu().numpy()
+        ref = orc.dijkstra(hg.rowptr, hg.colind, hg.fweights, s)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (kind, method, s)
+        assert orc.validate_spt(hg.rowptr, hg.colind, hg.fweights, s, got, p.cpu().numpy()) == 0
+        d2, _, _ = g.sssp(s, method=method)
+        assert np.array_equal(d2.cpu().numpy().view(np.uint32), got.view(np.uint32))
+    g.close()
+
+
+@pytest.mark.parametrize("method", ["delta", "adds", "bf"])
+def test_budget_runs_out_then_next_solve_is_exact(b2, orc, cuda, method):
+    from b200sssp import _lib
+    hg = b2.gen_rmat(17, 16, 0.57, 0.19, 0.19, 1, 255, 8)
+    g = b2.Graph.from_host(hg, "u32")
+    with pytest.raises(_lib.B2Error) as ei:
+        g.sssp(3, method=method, timeout_ms=0.001)
+    assert ei.value.status == _lib.TIMEOUT
+    d, _, st = g.sssp(3, method=method)
+    assert np.array_equal(_u32(d), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 3))
+    g.close()
+
+
+@pytest.mark.parametrize("method", ["delta", "bf"])
+def test_worklist_capacity_overflow_is_pool_exhausted(b2, orc, cuda, method):
+    from b200sssp import _lib
+    hg = b2.gen_rmat(16, 16, 0.57, 0.19, 0.19, 1, 255, 9)
+    g = b2.Graph.from_host(hg, "u32")
+    with pytest.raises(_lib.B2Error) as ei:
+        g.sssp(1, method=method, worklist_capacity=64)
+    assert ei.value.status == _lib.POOL_EXHAUSTED
+    d, _, _ = g.sssp(1, method=method)
+    assert np.array_equal(_u32(d), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 1))
+    # a capacity the solve never reaches changes nothing
+    d, _, _ = g.sssp(1, method=method, worklist_capacity=hg.n - 1)
+    assert np.array_equal(_u32(d), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 1))
+    g.close()

@@ -200,3 +200,41 @@ def test_row_parallel_reference_bf_equals_the_serial_port(orc):
         got = orc.sssp_min_plus_bellman_ford_rows(A, 0)
         A.close()
         assert np.array_equal(got[0], want[0]) and got[1:] == want[1:]
+
+
+def test_warm_start_dijkstra(orc):
+    """Warm start (hip_adds::sssp, initialize_distances = false): the given
+    labels are upper bounds, only the source starts in the queue.  All-INF
+    labels give the cold solve; otherwise the result equals a FIFO
+    label-correcting run from the source alone (an order-free fixpoint)."""
+    from collections import deque
+    rng = np.random.default_rng(17)
+    n, m = 400, 2400
+    src = rng.integers(0, n, m)
+    dst = rng.integers(0, n, m)
+    w = rng.integers(1, 50, m).astype(np.uint32)
+    o = np.lexsort((dst, src))
+    src, dst, w = src[o], dst[o], w[o]
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, src + 1, 1)
+    rp = np.cumsum(rp)
+    ci = dst.astype(np.int32)
+    cold = orc.dijkstra(rp, ci, w, 0)
+    assert np.array_equal(orc.dijkstra_warm(rp, ci, w, 0, np.full(n, 0xFFFFFFFF, np.uint32)), cold)
+    init = np.full(n, 0xFFFFFFFF, np.uint32)
+    pick = rng.choice(n, 60, replace=False)
+    init[pick] = rng.integers(0, 200, 60).astype(np.uint32)
+    got = orc.dijkstra_warm(rp, ci, w, 0, init)
+    d = init.astype(np.int64)
+    d[d == 0xFFFFFFFF] = 1 << 40
+    d[0] = 0
+    q = deque([0])
+    while q:
+        u = q.popleft()
+        for e in range(rp[u], rp[u + 1]):
+            if d[u] + int(w[e]) < d[ci[e]]:
+                d[ci[e]] = d[u] + int(w[e])
+                q.append(int(ci[e]))
+    want = np.where(d >= 1 << 40, 0xFFFFFFFF, d).astype(np.uint32)
+    assert np.array_equal(got, want)
+    assert np.all(got <= np.where(np.arange(n) == 0, 0, init))
