@@ -115,6 +115,20 @@ typedef enum b2_bf_check {
   B2_BF_VAR_CHECKS = 2  /* convergence observed only every check_interval iterations */
 } b2_bf_check;
 
+/* Progress of a running solve, reported to b2_sssp_opts.progress from the
+ * calling thread while the persistent kernel runs (it publishes each finished
+ * round or bucket to mapped host memory; the call polls it).  The reference
+ * calls its BellmanFordCsrProgressCallback once per iteration from its host
+ * loop (bf_hip_CSR.cpp:79-95). */
+typedef struct b2_progress {
+  int32_t iteration;        /* BF: rounds finished; delta / ADDS: non-empty buckets settled */
+  int32_t max_iters;        /* the solve's limit (-1: none) */
+  int32_t changed;          /* BF: the round changed a distance; delta / ADDS: 1 */
+  int32_t reserved;
+  double elapsed_ms;        /* device time from the solve's start to the round's end */
+} b2_progress;
+typedef void (*b2_progress_fn)(const b2_progress* progress, void* user_data);
+
 typedef struct b2_sssp_opts {
   int32_t max_iters;        /* BF: rounds (<0: n-1).  delta: buckets (<0: unbounded). */
   int32_t bf_check;         /* b2_bf_check */
@@ -166,6 +180,9 @@ typedef struct b2_sssp_opts {
   int32_t adds_fixed_delta; /* ADDS: 1 keeps the bucket width fixed (the reference's
                                dynamic_delta = false); 0 (default): growth 1.5 / shrink 0.75 at
                                every new window from the last window's utilization */
+  b2_progress_fn progress;  /* nullable: called once per finished round / bucket, in order,
+                               while the solve runs (every call precedes the return) */
+  void* progress_user;
   int32_t reserved[3];
 } b2_sssp_opts;
 

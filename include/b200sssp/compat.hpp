@@ -104,8 +104,9 @@ struct HostCsrF32 {
 
 // Matrix convention: row v, column u = weight of edge u -> v (incoming).
 // The whole solve runs in one persistent launch; the progress callback is
-// replayed after it, once per iteration, with the same field values the
-// reference's per-iteration loop reports.
+// called from the calling thread while it runs, once per iteration and in
+// order, with the field values the reference's per-iteration loop reports
+// (rounds the reference would run after convergence follow at the end).
 BellmanFordCsrResult bellman_ford_minplus_hip_csr(const minplus_sparse::DeviceCsrF32& d_adjacency, int source,
                                                   int max_iters, cudaStream_t stream = nullptr,
                                                   BellmanFordCsrProgressCallback progress_callback = nullptr,

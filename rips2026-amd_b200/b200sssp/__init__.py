@@ -248,19 +248,32 @@ class Graph:
 
     def sssp(self, source: int, method: str = "delta", pred: bool = False, out=None, out_pred=None,
              stream=None, **opts):
-        """Run one solve; returns (dist tensor, pred tensor | None, stats dict)."""
+        """Run one solve; returns (dist tensor, pred tensor | None, stats dict).
+        opts are b2_sssp_opts fields; progress=callable(dict) is called once per
+        finished round (BF) or bucket (delta, ADDS) while the solve runs."""
         torch = _torch()
         dt = torch.float32 if self.weight == "f32" else torch.int32
         dist = out if out is not None else torch.empty(self.n, dtype=dt, device="cuda")
         pr = None
         if pred:
             pr = out_pred if out_pred is not None else torch.empty(self.n, dtype=torch.int32, device="cuda")
+        progress = opts.pop("progress", None)
         o = default_opts(**opts)
+        keep = None
+        if progress is not None:
+            # called from this thread while the kernel runs, once per round / bucket
+            def _cb(p, _user):
+                q = p.contents
+                progress({"iteration": q.iteration, "max_iters": q.max_iters, "changed": bool(q.changed),
+                          "elapsed_ms": q.elapsed_ms})
+            keep = _lib.PROGRESS_FN(_cb)
+            o.progress = C.cast(keep, C.c_void_p)
         st = _lib.Stats()
         fn = getattr(lib(), _METHODS[method])
         check(fn(self._h, source, C.c_void_p(dist.data_ptr()),
                  C.c_void_p(pr.data_ptr() if pr is not None else 0), C.byref(o),
                  C.c_void_p(_stream_ptr(stream)), C.byref(st)), f"sssp[{method}]")
+        del keep
         return dist, pr, st.as_dict()
 
     def trace(self) -> list[dict]:

@@ -53,7 +53,16 @@ class Opts(C.Structure):
                 ("timeout_ms", C.c_double), ("collect_reach", C.c_int32),
                 ("detect_negative_cycle", C.c_int32), ("light_heavy", C.c_int32), ("trace", C.c_int32),
                 ("dense_fraction", C.c_float), ("worklist_capacity", C.c_uint32), ("keep_distances", C.c_int32),
-                ("active_buckets", C.c_uint32), ("adds_fixed_delta", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("active_buckets", C.c_uint32), ("adds_fixed_delta", C.c_int32), ("progress", C.c_void_p),
+                ("progress_user", C.c_void_p), ("reserved", C.c_int32 * 3)]
+
+
+class Progress(C.Structure):
+    _fields_ = [("iteration", C.c_int32), ("max_iters", C.c_int32), ("changed", C.c_int32),
+                ("reserved", C.c_int32), ("elapsed_ms", C.c_double)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.POINTER(Progress), C.c_void_p)
 
 
 class TraceEntry(C.Structure):

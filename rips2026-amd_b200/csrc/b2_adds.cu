@@ -96,6 +96,7 @@ struct AParams {
   uint32_t dist_is_out;
   const uint32_t* perm;    // degree-ordered graph: internal -> input id
   const uint32_t* inv;     // input -> internal id
+  ProgressBoard* board;    // mapped progress record (null: no progress callback)
 };
 
 // The epoch a warp works in; stable while the warp holds claimed work.
@@ -598,7 +599,9 @@ __device__ void idle_step(const AParams& P) {
     if (atomicCAS(&c->head, h, h + 1) == h) {
       const uint32_t r = ld_vol(&c->slot[h].reserved);
       if (r) {
-        atomicAdd(&c->buckets, 1u);
+        const uint32_t nb = atomicAdd(&c->buckets, 1u) + 1;
+        // buckets before this one had a successor; the last is reported at the end
+        if (nb > 1) publish_progress(P.board, nb - 1, 1u, globaltimer_ns() - ld_vol64(&c->t_start));
         atomicAdd(&c->epoch_buckets, 1u);
         atomicAdd(&c->epoch_entries, (unsigned long long)r);
         trace_bucket(P, h, ld_vol(&c->W) + h);
@@ -956,6 +959,8 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
     B2_CUDA_TRY(cudaMemsetAsync(w.adds_hub, 0xFF, w.adds_hub_cap * sizeof(unsigned long long), st));
   }
   B2_CUDA_TRY(cudaMemsetAsync(w.adds_ctl, 0, sizeof(AddsControl), st));
+  s = progress_begin(g, o, &P.board);
+  if (s != B2_SUCCESS) return s;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -965,6 +970,8 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   else e = pred ? launch_adds<WU32, true>(P, grid, st) : launch_adds<WU32, false>(P, grid, st);
   cudaEventRecord(e1, st);
   if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return from_cuda(e); }
+  uint32_t reported = 0;
+  if (P.board) progress_poll(g, o, e1, -1, &reported);
   e = cudaMemcpyAsync(w.adds_h_ctl, w.adds_ctl, sizeof(AddsControl), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   float ms = 0.0f;
@@ -973,6 +980,7 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return from_cuda(e);
   const AddsControl& hc = *w.adds_h_ctl;
+  if (P.board) progress_finish(g, o, -1, hc.buckets, hc.converged ? 0 : 1, &reported);
   w.adds_dirty = hc.error != kErrNone;
   w.trace_n = o.trace ? std::min<uint32_t>(hc.trace_n, kTraceCap) : 0;
   if (stats) {

@@ -5,8 +5,8 @@
 //   Charlotte_oneshot/sssp_hip.cpp:25-81 and 350-595,
 //   jasper_oneshot_untested/hip_adds_sssp.cpp:1138-1301,
 //   minplus_hip.cpp:122-173, minplus_sparse_hip.cpp:410-813.
-// The solves themselves run in one persistent launch each; per-iteration
-// progress callbacks are replayed afterwards from the solve's counts.
+// The solves themselves run in one persistent launch each; progress callbacks
+// are called from the calling thread while the kernel runs (b2_progress).
 #include "../../include/b200sssp/compat.hpp"
 
 #include <chrono>
@@ -95,14 +95,59 @@ b2_graph incoming_graph(const HostCsrF32& h, int source, cudaStream_t st) {
   return g;
 }
 
+// Live progress: the C ABI calls this bridge from the calling thread while
+// the persistent kernel runs (one call per finished round / bucket, in
+// order); it forwards each call in the reference's callback form.  Rounds
+// the reference would still run after the kernel has converged (no-checks
+// and var-checks loops) change nothing and are reported after the solve.
+struct Bridge {
+  enum Kind { kChecked, kNoChecks, kVarChecks, kDelta };
+  BellmanFordCsrProgressCallback cb = nullptr;
+  void* ud = nullptr;
+  Kind kind = kChecked;
+  int interval = 1;
+  int max_iters = 0;
+  int reported = 0;
+
+  void emit(int iteration, bool changed) {
+    BellmanFordCsrProgress q;
+    q.iteration = iteration;
+    q.max_iters = max_iters;
+    switch (kind) {
+      case kNoChecks:
+        q.convergence_checked = false;
+        q.changed = false;
+        break;
+      case kVarChecks:
+        q.convergence_checked = (iteration % interval) == 0;
+        q.changed = q.convergence_checked && changed;
+        break;
+      default:
+        q.convergence_checked = true;
+        q.changed = changed;
+    }
+    cb(q, ud);
+    reported = iteration;
+  }
+  void finish(int total) {   // rounds after the kernel converged: nothing changes
+    if (cb)
+      while (reported < total) emit(reported + 1, false);
+  }
+};
+
+extern "C" void compat_progress_bridge(const b2_progress* p, void* user) {
+  static_cast<Bridge*>(user)->emit(p->iteration, p->changed != 0);
+}
+
 struct BfRun {
   std::vector<float> dist;
   b2_stats st{};
   int max_iters = 0;
   double kernel_ms = 0, init_ms = 0, copy_ms = 0;
+  std::vector<double> round_end_ms;   // device time at the end of each round (traced solves)
 };
 
-BfRun run_bf(b2_graph g, int n, int source, int max_iters, cudaStream_t stream) {
+BfRun run_bf(b2_graph g, int n, int source, int max_iters, cudaStream_t stream, Bridge* bridge, bool trace) {
   using clk = std::chrono::steady_clock;
   BfRun r;
   r.max_iters = max_iters < 0 ? n - 1 : max_iters;
@@ -112,6 +157,12 @@ BfRun run_bf(b2_graph g, int n, int source, int max_iters, cudaStream_t stream) 
   b2_sssp_opts o;
   b2_sssp_opts_default(&o);
   o.max_iters = r.max_iters;
+  o.trace = trace ? 1 : 0;
+  if (bridge && bridge->cb) {
+    bridge->max_iters = r.max_iters;
+    o.progress = compat_progress_bridge;
+    o.progress_user = bridge;
+  }
   throw_status(b2_sssp_bf(g, (uint32_t)source, d.p, nullptr, &o, stream, &r.st), "bellman-ford");
   const auto t2 = clk::now();
   r.dist = to_host(d.p, (size_t)n, stream);
@@ -119,6 +170,19 @@ BfRun run_bf(b2_graph g, int n, int source, int max_iters, cudaStream_t stream) 
   r.init_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   r.kernel_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
   r.copy_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
+  if (trace) {
+    std::vector<b2_trace_entry> tr(4096);
+    int32_t cnt = 0;
+    if (b2_graph_trace(g, tr.data(), (int32_t)tr.size(), &cnt) == B2_SUCCESS) {
+      // the phases of round i carry bucket == i; its end is its last phase's end
+      for (int32_t k = 0; k < cnt; ++k) {
+        const uint32_t round = tr[k].bucket;
+        if (round == 0 || round > (uint32_t)r.max_iters) continue;
+        if (r.round_end_ms.size() < round) r.round_end_ms.resize(round, 0.0);
+        r.round_end_ms[round - 1] = std::max(r.round_end_ms[round - 1], (double)tr[k].t_ns * 1e-6);
+      }
+    }
+  }
   return r;
 }
 
@@ -129,40 +193,30 @@ bool round_changed(const b2_stats& st, int i) {
 
 BellmanFordCsrResult bf_checked(b2_graph g, int n, int source, int max_iters, cudaStream_t stream,
                                 BellmanFordCsrProgressCallback cb, void* ud) {
-  BfRun r = run_bf(g, n, source, max_iters, stream);
+  Bridge br;
+  br.cb = cb;
+  br.ud = ud;
+  br.kind = Bridge::kChecked;
+  BfRun r = run_bf(g, n, source, max_iters, stream, &br, false);
   BellmanFordCsrResult res;
   res.dist = std::move(r.dist);
   res.iterations_used = r.st.iterations_used;
   res.converged = r.st.converged != 0;
-  if (cb) {
-    for (int i = 1; i <= res.iterations_used; ++i) {
-      BellmanFordCsrProgress p;
-      p.iteration = i;
-      p.max_iters = r.max_iters;
-      p.convergence_checked = true;
-      p.changed = round_changed(r.st, i);
-      cb(p, ud);
-    }
-  }
+  br.finish(res.iterations_used);
   return res;
 }
 
 BellmanFordCsrNoChecksResult bf_no_checks(b2_graph g, int n, int source, int max_iters, cudaStream_t stream,
                                           BellmanFordCsrProgressCallback cb, void* ud) {
-  BfRun r = run_bf(g, n, source, max_iters, stream);
+  Bridge br;
+  br.cb = cb;
+  br.ud = ud;
+  br.kind = Bridge::kNoChecks;
+  BfRun r = run_bf(g, n, source, max_iters, stream, &br, false);
   BellmanFordCsrNoChecksResult res;
   res.dist = std::move(r.dist);
   res.iterations_used = r.max_iters;   // rounds after convergence change nothing
-  if (cb) {
-    for (int i = 1; i <= r.max_iters; ++i) {
-      BellmanFordCsrProgress p;
-      p.iteration = i;
-      p.max_iters = r.max_iters;
-      p.convergence_checked = false;
-      p.changed = false;
-      cb(p, ud);
-    }
-  }
+  br.finish(r.max_iters);
   return res;
 }
 
@@ -171,7 +225,12 @@ BellmanFordCsrVarChecksResult bf_var_checks(b2_graph g, int n, int source, int m
   if (check_interval <= 0) throw std::invalid_argument("check_interval must be positive");
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
-  BfRun r = run_bf(g, n, source, max_iters, stream);
+  Bridge br;
+  br.cb = cb;
+  br.ud = ud;
+  br.kind = Bridge::kVarChecks;
+  br.interval = check_interval;
+  BfRun r = run_bf(g, n, source, max_iters, stream, &br, true);
   BellmanFordCsrVarChecksResult res;
   res.dist = std::move(r.dist);
   res.check_interval = check_interval;
@@ -195,21 +254,25 @@ BellmanFordCsrVarChecksResult bf_var_checks(b2_graph g, int n, int source, int m
   res.initialization_ms = r.init_ms;
   res.relaxation_ms = r.st.kernel_ms;
   res.bellman_ford_loop_ms = r.kernel_ms;
-  res.checked_iteration_ms = res.checks_performed ? r.kernel_ms * res.checks_performed / res.iterations_used : 0;
-  res.unchecked_iteration_ms = r.kernel_ms - res.checked_iteration_ms;
+  // checked / unchecked round time from the kernel's own per-phase clock
+  // (bf_var_checks.cpp:70-186 times them on the host); rounds the kernel did
+  // not run (after convergence) took no time
+  double checked = 0.0, unchecked = 0.0, prev = 0.0;
+  for (size_t i = 0; i < r.round_end_ms.size(); ++i) {
+    const double end = std::max(prev, r.round_end_ms[i]);
+    const double dur = end - prev;
+    prev = end;
+    if ((int)(i + 1) > res.iterations_used) break;
+    if ((int)(i + 1) % check_interval == 0) checked += dur;
+    else unchecked += dur;
+  }
+  if (r.round_end_ms.empty()) unchecked = r.st.kernel_ms;
+  res.checked_iteration_ms = checked;
+  res.unchecked_iteration_ms = unchecked;
   res.final_copy_ms = r.copy_ms;
   res.estimated_check_overhead_ms = 0.0;   // change detection is free on the device
   res.total_runtime_ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-  if (cb) {
-    for (int i = 1; i <= res.iterations_used; ++i) {
-      BellmanFordCsrProgress p;
-      p.iteration = i;
-      p.max_iters = r.max_iters;
-      p.convergence_checked = (i % check_interval) == 0;
-      p.changed = p.convergence_checked ? round_changed(r.st, i) : false;
-      cb(p, ud);
-    }
-  }
+  br.finish(res.iterations_used);
   return res;
 }
 
@@ -233,6 +296,15 @@ DeltaSteppingCsrResult delta_run(b2_graph g, int n, int source, float delta, int
   o.delta = (double)delta;
   o.max_iters = max_iters;   // < 0: unbounded (delta_stepping_hip_CSR.cpp:666)
   o.light_heavy = 1;
+  Bridge br;
+  br.cb = cb;
+  br.ud = ud;
+  br.kind = Bridge::kDelta;
+  br.max_iters = max_iters < 0 ? std::numeric_limits<int>::max() : max_iters;
+  if (cb) {
+    o.progress = compat_progress_bridge;
+    o.progress_user = &br;
+  }
   b2_stats st;
   const b2_status s = b2_sssp_delta(g, (uint32_t)source, d.p, nullptr, &o, stream, &st);
   if (s == B2_INVALID_WEIGHT)
@@ -242,17 +314,6 @@ DeltaSteppingCsrResult delta_run(b2_graph g, int n, int source, float delta, int
   res.dist = to_host(d.p, (size_t)n, stream);
   res.iterations_used = st.iterations_used;
   res.converged = st.converged != 0;
-  if (cb) {
-    const int mi = max_iters < 0 ? std::numeric_limits<int>::max() : max_iters;
-    for (int i = 1; i <= res.iterations_used; ++i) {
-      DeltaSteppingCsrProgress p;
-      p.iteration = i;
-      p.max_iters = mi;
-      p.convergence_checked = true;
-      p.changed = !(res.converged && i == res.iterations_used);
-      cb(p, ud);
-    }
-  }
   return res;
 }
 

@@ -436,6 +436,7 @@ b2_status ensure_workspace(b2_graph g, bool pred) {
   fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   free_adds_workspace(w);
+  if (w.board_h) cudaFreeHost(w.board_h);
   w = Workspace();
   const size_t word = pred ? 8 : 4;
   w.n = n;
@@ -590,6 +591,7 @@ extern "C" b2_status b2_graph_destroy(b2_graph g) {
   fr(w.ctl); fr(w.reach);
   if (w.h_ctl) cudaFreeHost(w.h_ctl);
   free_adds_workspace(w);
+  if (w.board_h) cudaFreeHost(w.board_h);
   delete g;
   return B2_SUCCESS;
 }

@@ -156,6 +156,15 @@ struct Control {
   unsigned long long pushes;
 };
 
+// Progress record in mapped host memory.  The solve's manager step writes it
+// after every finished round / bucket (`rounds` last, with a system-scope
+// release); the calling thread polls it while the kernel runs.
+struct ProgressBoard {
+  uint32_t rounds;
+  uint32_t changed;
+  unsigned long long t_ns;   // end of the round, ns after the solve's start
+};
+
 // ---- asynchronous ADDS worklist (b2_adds.cu) ------------------------------
 // Buckets of one window epoch: slot s holds global bucket W + s.  Each slot is
 // an append-only queue with its own counters on a 128-byte line.
@@ -242,6 +251,8 @@ struct Workspace {
   unsigned long long* reach = nullptr;   // [reached vertices, their out-edges] of the last solve
   uint32_t phase_epoch = 0;
   size_t bytes = 0;
+  ProgressBoard* board_h = nullptr;  // mapped pinned progress record (first solve with a callback)
+  ProgressBoard* board_d = nullptr;  // its device address
   // ADDS worklist (allocated on the first b2_sssp_adds solve)
   uint32_t* adds_q = nullptr;       // (kAddsSlots + 2) queues of adds_cap entries: window slots, 2 far piles
   size_t adds_cap = 0;
@@ -292,6 +303,13 @@ void free_adds_workspace(Workspace& w);
 // Asynchronous ADDS worklist solve (b2_adds.cu).
 b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, const b2_sssp_opts* o,
                    cudaStream_t st, b2_stats* stats);
+// Live progress: prepare the board before a launch (null when no callback),
+// then poll it until `done` has completed, calling o.progress for each new
+// round in order; finish_progress reports what the kernel published last.
+b2_status progress_begin(b2_graph g, const b2_sssp_opts& o, ProgressBoard** board_d);
+void progress_poll(b2_graph g, const b2_sssp_opts& o, cudaEvent_t done, int32_t max_iters, uint32_t* reported);
+void progress_finish(b2_graph g, const b2_sssp_opts& o, int32_t max_iters, uint32_t final_rounds, int32_t last_changed,
+                     uint32_t* reported);
 // stats->reached / reached_edges from a solve's labels (keys, or key|pred words when pred).
 b2_status collect_reach(b2_graph g, const void* labels, bool pred, bool isf, cudaStream_t st, b2_stats* stats);
 b2_status ensure_incoming(b2_graph g, cudaStream_t st);

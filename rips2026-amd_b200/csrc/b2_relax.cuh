@@ -8,8 +8,20 @@
 #include <stdint.h>
 
 #include "b2_common.cuh"
+#include "b2_internal.hpp"
 
 namespace b2 {
+
+// Publish a finished round / bucket to the mapped progress record (one
+// thread; `rounds` is stored last with a system-scope release).
+__device__ __forceinline__ void publish_progress(ProgressBoard* b, uint32_t rounds, uint32_t changed,
+                                                 unsigned long long t_ns) {
+  if (!b) return;
+  *(volatile uint32_t*)&b->changed = changed;
+  *(volatile unsigned long long*)&b->t_ns = t_ns;
+  __threadfence_system();
+  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(&b->rounds), "r"(rounds) : "memory");
+}
 
 // ---------------------------------------------------------------------------
 // label access

@@ -42,8 +42,11 @@
 // which at least one vertex was settled, exactly the reference's count of
 // outer iterations.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "b2_common.cuh"
@@ -107,6 +110,7 @@ struct Params {
   uint32_t adapt_cap;     // ADDS: frontier entries the grid takes per phase (utilization base)
   uint32_t dense_min;     // delta: near / slot frontiers of at least this many entries are swept
   uint32_t qcap;          // entries each worklist queue may hold (<= n; a push past it is kErrQueueOverflow)
+  ProgressBoard* board;   // mapped progress record (null: no progress callback)
 };
 
 // Bucket of a distance key under the phase's mapping
@@ -855,6 +859,7 @@ __device__ void manager_bf(const Params& P) {
     return;
   }
   c->iterations = r.iter;
+  publish_progress(P.board, r.iter, changed ? 1u : 0u, globaltimer_ns() - c->t_start);
   if (!changed) {
     c->converged = 1;
     c->first_unchanged = r.iter;
@@ -996,6 +1001,9 @@ __device__ void manager_delta(const Params& P) {
     if (vld(&c->bucket_valid)) {
       c->iterations = vld(&c->iterations) + 1;
       c->bucket_valid = 0;
+      // the previous bucket had a successor (the reference's `changed`,
+      // delta_stepping_hip_CSR.cpp:744-756); the last one is reported at the end
+      if (c->iterations > 1) publish_progress(P.board, c->iterations - 1, 1u, globaltimer_ns() - c->t_start);
     }
     if (vld(&c->iterations) >= P.max_iters) {
       nx.kind = kPhaseProbe;
@@ -1403,6 +1411,60 @@ b2_status ensure_in_light_counts(b2_graph g, bool isf, uint32_t delta_u, float d
   return B2_SUCCESS;
 }
 
+b2_status progress_begin(b2_graph g, const b2_sssp_opts& o, ProgressBoard** board_d) {
+  *board_d = nullptr;
+  if (!o.progress) return B2_SUCCESS;
+  Workspace& w = g->ws;
+  if (!w.board_h) {
+    B2_CUDA_TRY(cudaHostAlloc((void**)&w.board_h, sizeof(ProgressBoard), cudaHostAllocMapped));
+    cudaError_t e = cudaHostGetDevicePointer((void**)&w.board_d, w.board_h, 0);
+    if (e != cudaSuccess) {
+      cudaFreeHost(w.board_h);
+      w.board_h = nullptr;
+      return from_cuda(e);
+    }
+  }
+  *(volatile uint32_t*)&w.board_h->rounds = 0;
+  *(volatile uint32_t*)&w.board_h->changed = 0;
+  *(volatile unsigned long long*)&w.board_h->t_ns = 0;
+  *board_d = w.board_d;
+  return B2_SUCCESS;
+}
+
+namespace {
+void report_upto(const b2_sssp_opts& o, int32_t max_iters, uint32_t upto, uint32_t last_changed, double ms,
+                 uint32_t* reported) {
+  while (*reported < upto) {
+    ++*reported;
+    b2_progress p;
+    p.iteration = (int32_t)*reported;
+    p.max_iters = max_iters;
+    p.changed = (*reported < upto) ? 1 : (int32_t)last_changed;   // every round before the last one changed
+    p.reserved = 0;
+    p.elapsed_ms = ms;
+    o.progress(&p, o.progress_user);
+  }
+}
+}  // namespace
+
+void progress_poll(b2_graph g, const b2_sssp_opts& o, cudaEvent_t done, int32_t max_iters, uint32_t* reported) {
+  const volatile ProgressBoard* b = g->ws.board_h;
+  for (;;) {
+    const cudaError_t q = cudaEventQuery(done);
+    const uint32_t r = b->rounds;
+    std::atomic_thread_fence(std::memory_order_acquire);
+    if (r > *reported) report_upto(o, max_iters, r, b->changed, (double)b->t_ns * 1e-6, reported);
+    if (q != cudaErrorNotReady) return;
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
+void progress_finish(b2_graph g, const b2_sssp_opts& o, int32_t max_iters, uint32_t final_rounds, int32_t last_changed,
+                     uint32_t* reported) {
+  const volatile ProgressBoard* b = g->ws.board_h;
+  report_upto(o, max_iters, final_rounds, (uint32_t)last_changed, (double)b->t_ns * 1e-6, reported);
+}
+
 b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t* d_pred,
                    const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats, bool adds = false) {
   if (!g || !d_dist) return B2_INVALID_ARGUMENT;
@@ -1554,6 +1616,8 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   }
   P.phase_base = w.phase_epoch;
 
+  s = progress_begin(g, o, &P.board);
+  if (s != B2_SUCCESS) return s;
   int grid = 0;
   cudaError_t e = cudaSuccess;
   B2_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(Control), st));
@@ -1577,6 +1641,9 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
 #undef B2_LAUNCH
   cudaEventRecord(e1, st);
   if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return from_cuda(e); }
+  const int32_t prog_max = mode == kModeBF ? (int32_t)P.max_iters : (o.max_iters < 0 ? -1 : o.max_iters);
+  uint32_t reported = 0;
+  if (P.board) progress_poll(g, o, e1, prog_max, &reported);
   e = cudaMemcpyAsync(w.h_ctl, w.ctl, sizeof(Control), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   float ms = 0.0f;
@@ -1585,6 +1652,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return from_cuda(e);
   const Control& hc = *w.h_ctl;
+  if (P.board) progress_finish(g, o, prog_max, hc.iterations, hc.converged ? 0 : 1, &reported);
   w.phase_epoch += std::max(hc.rec.phase, hc.stamp_ctr) + 2;
   w.trace_n = o.trace ? hc.trace_n : 0;
   b2_status ds = map_device_error(hc.error);

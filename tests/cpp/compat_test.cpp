@@ -175,6 +175,29 @@ int main() {
     for (int i = 0; i < n && ok; ++i) ok = std::isinf(refu[i]) ? hd[i] == 0xFFFFFFFFu : (float)hd[i] == refu[i];
     check(ok, std::string("hip_adds::sssp uint32 exact (") + hip_adds::status_string(st) + ")");
     check(hip_adds::sssp(dg, n + 1, dd) == hip_adds::Status::InvalidArgument, "hip_adds::sssp bad source");
+    // warm start (initialize_distances = false): upper bounds above the answer
+    // are all improved back to it; the answer itself is kept as it is
+    hip_adds::Options warm;
+    warm.initialize_distances = false;
+    for (int round = 0; round < 2; ++round) {
+      std::vector<uint32_t> start(hd);
+      if (round == 0)
+        for (int i = 0; i < n; ++i) start[i] = start[i] == 0xFFFFFFFFu ? start[i] : start[i] + 5u;
+      cudaMemcpy(dd, start.data(), (size_t)n * 4, cudaMemcpyHostToDevice);
+      st = hip_adds::sssp(dg, 0, dd, &rs, warm);
+      std::vector<uint32_t> hw(n);
+      cudaMemcpy(hw.data(), dd, (size_t)n * 4, cudaMemcpyDeviceToHost);
+      check(st == hip_adds::Status::Success && hw == hd,
+            round == 0 ? "hip_adds::sssp warm start from raised bounds" : "hip_adds::sssp warm start from the answer");
+    }
+    hip_adds::Options fixed;
+    fixed.dynamic_delta = false;
+    fixed.initial_delta = 7.0;
+    st = hip_adds::sssp(dg, 0, dd, &rs, fixed);
+    std::vector<uint32_t> hf(n);
+    cudaMemcpy(hf.data(), dd, (size_t)n * 4, cudaMemcpyDeviceToHost);
+    check(st == hip_adds::Status::Success && hf == hd && rs.delta_updates == 0 && rs.final_delta == 7.0,
+          "hip_adds::sssp fixed delta");
     cudaFree(drp); cudaFree(dci); cudaFree(dw); cudaFree(dd);
   }
 

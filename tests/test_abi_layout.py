@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _pairs():
     from b200sssp import _lib, serving
     return {"b2_csr": _lib.CSR, "b2_graph_info": _lib.GraphInfo, "b2_sssp_opts": _lib.Opts,
-            "b2_trace_entry": _lib.TraceEntry, "b2_stats": _lib.Stats, "b2_host_csr": _lib.HostCSR,
+            "b2_trace_entry": _lib.TraceEntry, "b2_progress": _lib.Progress, "b2_stats": _lib.Stats, "b2_host_csr": _lib.HostCSR,
             "b2_server_opts": serving.ServerOpts, "b2_completion": serving.Completion,
             "b2_server_info_t": serving.ServerInfo, "b2_load_opts": serving.LoadOpts,
             "b2_load_report": serving.LoadReport}

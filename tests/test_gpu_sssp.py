@@ -495,3 +495,31 @@ def test_reference_tiny_lonestar_known_answer(b2, cuda):
         d, _, st = g.sssp(t["source"], method=method)
         assert np.array_equal(_np(d), exp), method
     g.close()
+
+
+@pytest.mark.parametrize("method", ["bf", "delta", "adds"])
+def test_live_progress_callback(b2, orc, cuda, method):
+    """The progress callback runs while the kernel runs: one call per round
+    (BF) or bucket (delta, ADDS), in order, the first well before the solve
+    returns; BF's last round reports no change (bf_hip_CSR.cpp:79-95), and
+    delta-stepping's last bucket reports no successor."""
+    import time
+    hg = b2.gen_grid(512, 512, 0.0, seed=77)
+    g = _graph(b2, hg, "u32")
+    g.sssp(0, method=method)   # warm: workspace, light counts
+    calls = []
+    t0 = time.perf_counter()
+    d, _, st = g.sssp(0, method=method, progress=lambda p: calls.append((time.perf_counter(), p)))
+    t1 = time.perf_counter()
+    assert np.array_equal(_dist_u32(d), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 0))
+    its = [p["iteration"] for _, p in calls]
+    assert its == list(range(1, st["iterations_used"] + 1))
+    assert all(p["changed"] for _, p in calls[:-1]) and not calls[-1][1]["changed"]
+    ms = [p["elapsed_ms"] for _, p in calls[:-1]]
+    assert all(a <= b for a, b in zip(ms, ms[1:]))
+    if method == "bf":
+        assert len(calls) > 100
+        # published while running: the first report precedes the return by
+        # a good part of the solve
+        assert calls[0][0] - t0 < 0.5 * (t1 - t0)
+    g.close()
