@@ -316,6 +316,20 @@ b2_status b2_minplus_spgemm_f32(const b2_csr* A, const b2_csr* B, int64_t** dC_r
 b2_status b2_minplus_spgemm_i32(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr,
                                 int32_t** dC_colind, int32_t** dC_values, int64_t* hC_nnz,
                                 b2_stream stream);
+/* The same product in two steps, for callers that allocate C themselves (no
+ * reference counterpart).  b2_minplus_spgemm_plan computes C into library
+ * scratch (stream-ordered pool memory) and returns nnz(C) on the host; the
+ * caller allocates C.rowptr (rows + 1 int64), C.colind (nnz int32) and
+ * C.values (nnz, A's weight type: float or int32), and b2_minplus_spgemm_fill
+ * writes them asynchronously on `stream` and releases the plan.
+ * b2_minplus_spgemm_plan_free releases a plan that is not filled.  A and B
+ * must have the same weight_type. */
+typedef struct b2_spgemm_plan_s* b2_spgemm_plan;
+b2_status b2_minplus_spgemm_plan(const b2_csr* A, const b2_csr* B, b2_stream stream, b2_spgemm_plan* plan,
+                                 int64_t* hC_nnz);
+b2_status b2_minplus_spgemm_fill(b2_spgemm_plan plan, int64_t* dC_rowptr, int32_t* dC_colind, void* dC_values,
+                                 b2_stream stream);
+b2_status b2_minplus_spgemm_plan_free(b2_spgemm_plan plan);
 
 /* ---- learned schedule policy -------------------------------------------
  * No counterpart in the reference (it picks delta with the Near-Far rule,

@@ -121,6 +121,9 @@ _SIGS = {
                                         C.POINTER(_P), C.POINTER(C.c_int64), _P]),
     "b2_minplus_spgemm_i32": (C.c_int, [C.POINTER(CSR), C.POINTER(CSR), C.POINTER(_P), C.POINTER(_P),
                                         C.POINTER(_P), C.POINTER(C.c_int64), _P]),
+    "b2_minplus_spgemm_plan": (C.c_int, [C.POINTER(CSR), C.POINTER(CSR), _P, C.POINTER(_P), C.POINTER(C.c_int64)]),
+    "b2_minplus_spgemm_fill": (C.c_int, [_P, _P, _P, _P, _P]),
+    "b2_minplus_spgemm_plan_free": (C.c_int, [_P]),
     "b2_policy_param_count": (C.c_int32, []),
     "b2_policy_create": (C.c_int, [C.c_uint64, C.POINTER(_P)]),
     "b2_policy_destroy": (C.c_int, [_P]),

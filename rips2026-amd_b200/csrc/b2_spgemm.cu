@@ -25,7 +25,9 @@
 //                    (k_expand, CUB segmented sort, k_compress into the same
 //                    scratch slots);
 //   5. scan of the counts (CUB) -> C.rowptr, then k_compact copies every row
-//      from its scratch slot to the exact-size outputs.
+//      from its scratch slot to the exact-size outputs: memory this call
+//      allocates (the reference's one-call form), or the caller's own buffers
+//      (b2_minplus_spgemm_plan / _fill, which need no output allocation here).
 // Scratch arrays come from a library-owned stream-ordered memory pool that
 // keeps up to 4 GiB cached between calls (no cudaMalloc / cudaFree on the
 // critical path after the first call).
@@ -416,16 +418,45 @@ struct DBuf {
     if (e != cudaSuccess) return e;
     return cudaMallocFromPoolAsync((void**)&p, std::max<size_t>(n, 1) * sizeof(T), pool, s);
   }
+  T* release() {
+    T* q = p;
+    p = nullptr;
+    return q;
+  }
 };
 
+}  // namespace
+
+// A computed product waiting for its outputs: every row's result sits in a
+// scratch slot (off[i] .. off[i] + cnt[i]) and crp holds C's row pointers.
+struct SpPlan {
+  int64_t M = 0;
+  int64_t nnz = 0;
+  int wt = B2_W_F32;
+  int64_t* crp = nullptr;            // pool memory
+  unsigned long long* off = nullptr; // pool memory
+  int32_t* tcol = nullptr;           // pool memory
+  void* tval = nullptr;              // pool memory
+  cudaStream_t st = nullptr;
+  void release() {
+    if (crp) cudaFreeAsync(crp, st);
+    if (off) cudaFreeAsync(off, st);
+    if (tcol) cudaFreeAsync(tcol, st);
+    if (tval) cudaFreeAsync(tval, st);
+    crp = nullptr;
+    off = nullptr;
+    tcol = nullptr;
+    tval = nullptr;
+  }
+};
+
+namespace {
+
+// Steps 1-5 up to C's row pointers; one host synchronization for the scratch
+// size (two when long rows exist) and one for nnz(C).
 template <typename T>
-b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t** dC_colind, T** dC_values,
-                 int64_t* hC_nnz, cudaStream_t st) {
-  if (!A || !B || !dC_rowptr || !dC_colind || !dC_values || !hC_nnz) return B2_INVALID_ARGUMENT;
-  *dC_rowptr = nullptr;
-  *dC_colind = nullptr;
-  *dC_values = nullptr;
-  *hC_nnz = 0;
+b2_status compute(const b2_csr* A, const b2_csr* B, cudaStream_t st, SpPlan& plan) {
+  if (!A || !B) return B2_INVALID_ARGUMENT;
   if (A->rows < 0 || A->cols < 0 || A->nnz < 0 || B->rows < 0 || B->cols < 0 || B->nnz < 0) return B2_INVALID_ARGUMENT;
   if (A->cols != B->rows) return B2_INVALID_ARGUMENT;
   if (A->cols > 0x7fffffffLL || B->cols > 0x7fffffffLL) return B2_INVALID_ARGUMENT;
@@ -436,17 +467,14 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
   const int64_t M = A->rows, K = A->cols, N = B->cols;
   const int64_t* arp = (const int64_t*)A->rowptr;
   const int64_t* brp = (const int64_t*)B->rowptr;
-  int64_t* crp = nullptr;
-  B2_CUDA_TRY(cudaMalloc((void**)&crp, (size_t)(M + 1) * sizeof(int64_t)));
-  auto fail = [&](b2_status s) {
-    cudaFree(crp);
-    return s;
-  };
+  plan.M = M;
+  plan.st = st;
+  DBuf<int64_t> crp;
+  if (crp.alloc((size_t)M + 1, st) != cudaSuccess) return B2_OUT_OF_MEMORY;
   if (M == 0 || K == 0 || A->nnz == 0 || B->nnz == 0) {
-    if (cudaMemsetAsync(crp, 0, (size_t)(M + 1) * sizeof(int64_t), st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return fail(B2_CUDA_ERROR);
-    *dC_rowptr = crp;
+    B2_CUDA_TRY(cudaMemsetAsync(crp.p, 0, (size_t)(M + 1) * sizeof(int64_t), st));
+    plan.crp = crp.release();
+    plan.nnz = 0;
     return B2_SUCCESS;
   }
   DBuf<unsigned long long> ub, off, lcount;
@@ -456,7 +484,7 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
   if (ub.alloc((size_t)M + 1, st) != cudaSuccess || off.alloc((size_t)M + 1, st) != cudaSuccess ||
       status.alloc(1, st) != cudaSuccess || lrows.alloc((size_t)M, st) != cudaSuccess ||
       lcount.alloc(1, st) != cudaSuccess)
-    return fail(B2_OUT_OF_MEMORY);
+    return B2_OUT_OF_MEMORY;
   cudaError_t e = cudaMemsetAsync(status.p, 0, 4, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ub.p + M, 0, 8, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(lcount.p, 0, 8, st);
@@ -475,9 +503,9 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hv[1], lcount.p, 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, status.p, 4, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return fail(from_cuda(e));
-  if (hs == kSpBadIndex) return fail(B2_INVALID_INDEX);
-  if (hs == kSpBadRowptr) return fail(B2_INVALID_ROWPTR);
+  if (e != cudaSuccess) return from_cuda(e);
+  if (hs == kSpBadIndex) return B2_INVALID_INDEX;
+  if (hs == kSpBadRowptr) return B2_INVALID_ROWPTR;
   const unsigned long long U = hv[0];
   const int64_t L = (int64_t)hv[1];
   DBuf<int32_t> tcol;
@@ -485,7 +513,7 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
   DBuf<int64_t> cnt;
   if (tcol.alloc(U, st) != cudaSuccess || tval.alloc(U, st) != cudaSuccess ||
       cnt.alloc((size_t)M + 1, st) != cudaSuccess)
-    return fail(B2_OUT_OF_MEMORY);
+    return B2_OUT_OF_MEMORY;
   if (U > 0) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -505,7 +533,7 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
   DBuf<unsigned char> tmp2, tmp3;
   if (e == cudaSuccess && L > 0) {
     if (lub.alloc((size_t)L + 1, st) != cudaSuccess || loff.alloc((size_t)L + 1, st) != cudaSuccess)
-      return fail(B2_OUT_OF_MEMORY);
+      return B2_OUT_OF_MEMORY;
     e = cudaMemsetAsync(lub.p + L, 0, 8, st);
     if (e == cudaSuccess) {
       k_long_bounds<<<(int)std::min<int64_t>((L + 255) / 256, 1184), 256, 0, st>>>(L, lrows.p, off.p, lub.p);
@@ -518,11 +546,11 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
     unsigned long long LU = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&LU, loff.p + L, 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return fail(from_cuda(e));
-    if (LU > 0x7fffffffull) return fail(B2_NOT_SUPPORTED);   // segmented sort item count is int
+    if (e != cudaSuccess) return from_cuda(e);
+    if (LU > 0x7fffffffull) return B2_NOT_SUPPORTED;   // segmented sort item count is int
     if (col0.alloc(LU, st) != cudaSuccess || col1.alloc(LU, st) != cudaSuccess || val0.alloc(LU, st) != cudaSuccess ||
         val1.alloc(LU, st) != cudaSuccess)
-      return fail(B2_OUT_OF_MEMORY);
+      return B2_OUT_OF_MEMORY;
     k_expand<T><<<grid_rows(L), 256, 0, st>>>(L, lrows.p, N, arp, A->colind, (const T*)A->values, brp, B->colind,
                                               (const T*)B->values, loff.p, col0.p, val0.p, status.p);
     e = cudaGetLastError();
@@ -542,37 +570,70 @@ b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t*
   if (e == cudaSuccess) e = cudaMemsetAsync(cnt.p + M, 0, 8, st);
   size_t tb4 = 0;
   DBuf<unsigned char> tmp4;
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb4, cnt.p, crp, M + 1, st);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb4, cnt.p, crp.p, M + 1, st);
   if (e == cudaSuccess) e = tmp4.alloc(tb4, st);
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp4.p, tb4, cnt.p, crp, M + 1, st);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp4.p, tb4, cnt.p, crp.p, M + 1, st);
   int64_t nnz = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&nnz, crp + M, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nnz, crp.p + M, 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, status.p, 4, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return fail(from_cuda(e));
-  if (hs == kSpBadIndex) return fail(B2_INVALID_INDEX);
-  if (hs == kSpBadRowptr) return fail(B2_INVALID_ROWPTR);
+  if (e != cudaSuccess) return from_cuda(e);
+  if (hs == kSpBadIndex) return B2_INVALID_INDEX;
+  if (hs == kSpBadRowptr) return B2_INVALID_ROWPTR;
+  plan.nnz = nnz;
+  plan.crp = crp.release();
+  plan.off = off.release();
+  plan.tcol = tcol.release();
+  plan.tval = tval.release();
+  return B2_SUCCESS;
+}
+
+// Scratch slots -> caller-visible outputs (stream-ordered).
+template <typename T>
+cudaError_t fill(const SpPlan& plan, int64_t* crp, int32_t* cci, T* cv, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(crp, plan.crp, (size_t)(plan.M + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess && plan.nnz > 0) {
+    k_compact<T><<<grid_rows(plan.M), 256, 0, st>>>(plan.M, plan.off, plan.crp, plan.tcol, (const T*)plan.tval,
+                                                    cci, cv);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+// The reference's one-call form: outputs cudaMalloc'd here, freed by the caller.
+template <typename T>
+b2_status spgemm(const b2_csr* A, const b2_csr* B, int64_t** dC_rowptr, int32_t** dC_colind, T** dC_values,
+                 int64_t* hC_nnz, cudaStream_t st) {
+  if (!dC_rowptr || !dC_colind || !dC_values || !hC_nnz) return B2_INVALID_ARGUMENT;
+  *dC_rowptr = nullptr;
+  *dC_colind = nullptr;
+  *dC_values = nullptr;
+  *hC_nnz = 0;
+  SpPlan plan;
+  b2_status s = compute<T>(A, B, st, plan);
+  if (s != B2_SUCCESS) {
+    plan.release();
+    return s;
+  }
+  int64_t* crp = nullptr;
   int32_t* cci = nullptr;
   T* cv = nullptr;
-  if (nnz > 0) {
-    if (cudaMalloc((void**)&cci, (size_t)nnz * sizeof(int32_t)) != cudaSuccess) return fail(B2_OUT_OF_MEMORY);
-    if (cudaMalloc((void**)&cv, (size_t)nnz * sizeof(T)) != cudaSuccess) {
-      cudaFree(cci);
-      return fail(B2_OUT_OF_MEMORY);
-    }
-    k_compact<T><<<grid_rows(M), 256, 0, st>>>(M, off.p, crp, tcol.p, tval.p, cci, cv);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-      cudaFree(cci);
-      cudaFree(cv);
-      return fail(from_cuda(e));
-    }
+  cudaError_t e = cudaMalloc((void**)&crp, (size_t)(plan.M + 1) * sizeof(int64_t));
+  if (e == cudaSuccess && plan.nnz > 0) e = cudaMalloc((void**)&cci, (size_t)plan.nnz * sizeof(int32_t));
+  if (e == cudaSuccess && plan.nnz > 0) e = cudaMalloc((void**)&cv, (size_t)plan.nnz * sizeof(T));
+  if (e == cudaSuccess) e = fill<T>(plan, crp, cci, cv, st);
+  plan.release();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    cudaFree(crp);
+    cudaFree(cci);
+    cudaFree(cv);
+    return e == cudaErrorMemoryAllocation ? B2_OUT_OF_MEMORY : from_cuda(e);
   }
   *dC_rowptr = crp;
   *dC_colind = cci;
   *dC_values = cv;
-  *hC_nnz = nnz;
+  *hC_nnz = plan.nnz;
   return B2_SUCCESS;
 }
 
@@ -591,4 +652,45 @@ extern "C" b2_status b2_minplus_spgemm_i32(const b2_csr* A, const b2_csr* B, int
                                            int32_t** dC_colind, int32_t** dC_values, int64_t* hC_nnz,
                                            b2_stream stream) {
   return b2::spgemm<int32_t>(A, B, dC_rowptr, dC_colind, dC_values, hC_nnz, (cudaStream_t)stream);
+}
+
+extern "C" b2_status b2_minplus_spgemm_plan(const b2_csr* A, const b2_csr* B, b2_stream stream,
+                                            b2_spgemm_plan* plan, int64_t* hC_nnz) {
+  if (!A || !B || !plan || !hC_nnz) return B2_INVALID_ARGUMENT;
+  *plan = nullptr;
+  *hC_nnz = 0;
+  if (A->weight_type != B->weight_type) return B2_INVALID_ARGUMENT;
+  b2::SpPlan* p = new b2::SpPlan();
+  p->wt = A->weight_type;
+  const b2_status s = A->weight_type == B2_W_F32 ? b2::compute<float>(A, B, (cudaStream_t)stream, *p)
+                                                  : b2::compute<int32_t>(A, B, (cudaStream_t)stream, *p);
+  if (s != B2_SUCCESS) {
+    p->release();
+    delete p;
+    return s;
+  }
+  *plan = reinterpret_cast<b2_spgemm_plan>(p);
+  *hC_nnz = p->nnz;
+  return B2_SUCCESS;
+}
+
+extern "C" b2_status b2_minplus_spgemm_fill(b2_spgemm_plan plan, int64_t* dC_rowptr, int32_t* dC_colind,
+                                            void* dC_values, b2_stream stream) {
+  b2::SpPlan* p = reinterpret_cast<b2::SpPlan*>(plan);
+  if (!p || !dC_rowptr || (p->nnz > 0 && (!dC_colind || !dC_values))) return B2_INVALID_ARGUMENT;
+  const cudaStream_t st = (cudaStream_t)stream;
+  p->st = st;   // scratch is released in the order of this stream
+  const cudaError_t e = p->wt == B2_W_F32 ? b2::fill<float>(*p, dC_rowptr, dC_colind, (float*)dC_values, st)
+                                          : b2::fill<int32_t>(*p, dC_rowptr, dC_colind, (int32_t*)dC_values, st);
+  p->release();
+  delete p;
+  return b2::from_cuda(e);
+}
+
+extern "C" b2_status b2_minplus_spgemm_plan_free(b2_spgemm_plan plan) {
+  b2::SpPlan* p = reinterpret_cast<b2::SpPlan*>(plan);
+  if (!p) return B2_INVALID_ARGUMENT;
+  p->release();
+  delete p;
+  return B2_SUCCESS;
 }

@@ -118,3 +118,29 @@ def test_spgemm_row_sizes_across_sort_widths(b2, orc, cuda, dtype):
     ref = orc.minplus_spgemm(A, B, N)
     for a, b in zip(got, ref):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "i32"])
+def test_plan_fill_equals_callee_allocated_form(b2, orc, cuda, dtype):
+    """The two-step form (b2_minplus_spgemm_plan / _fill into caller buffers)
+    and the reference's one-call form (library-allocated outputs) give the
+    same words; an unfilled plan is released by b2_minplus_spgemm_plan_free."""
+    torch = cuda
+    import ctypes as C
+    from b200sssp import _lib, minplus
+    hg = b2.gen_er(30000, 240000, 1, 1000, 91)
+    vals = hg.weights.view(np.int32) if dtype == "i32" else hg.weights.astype(np.float32) / np.float32(1001)
+    A = (torch.from_numpy(hg.rowptr).cuda(), torch.from_numpy(hg.colind).cuda(), torch.from_numpy(vals).cuda(), hg.n)
+    p1 = minplus.minplus_spgemm(A, A)
+    p2 = minplus.minplus_spgemm_callee_alloc(A, A)
+    for x, y in zip(p1, p2):
+        assert x.dtype == y.dtype and torch.equal(x, y)
+    ref = orc.minplus_spgemm((hg.rowptr, hg.colind, vals), (hg.rowptr, hg.colind, vals), hg.n)
+    assert np.array_equal(p1[0].cpu().numpy(), ref[0])
+    assert np.array_equal(p1[1].cpu().numpy(), ref[1])
+    assert np.array_equal(p1[2].cpu().numpy().view(np.uint32), ref[2].view(np.uint32))
+    a = minplus._csr_view(*A)
+    plan, nnz = C.c_void_p(), C.c_int64()
+    assert _lib.lib().b2_minplus_spgemm_plan(C.byref(a), C.byref(a), None, C.byref(plan), C.byref(nnz)) == 0
+    assert nnz.value == p1[1].numel()
+    assert _lib.lib().b2_minplus_spgemm_plan_free(plan) == 0
