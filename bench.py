@@ -776,9 +776,10 @@ def serve_measure(queries: int, rate: float, light_queries: int, seq_queries: in
     srv.run_load(256, rate_qps=0.0, seed=99, mode="server")                  # warm-up
     rep = srv.run_load(queries, rate_qps=rate, seed=SEED, mode="server")
     light = srv.run_load(light_queries, rate_qps=1000.0, seed=SEED + 1, mode="server")      # below capacity
+    heavy = srv.run_load(queries, rate_qps=50000.0, seed=SEED + 2, mode="server")           # the top of 1k-50k q/s
     seq = srv.run_load(seq_queries, rate_qps=0.0, seed=SEED, mode="sequential")
     srv.close()
-    out = {"server": rep, "light_load_1000qps": light, "sequential": seq,
+    out = {"server": rep, "light_load_1000qps": light, "heavy_load_50000qps": heavy, "sequential": seq,
            "speedup_over_sequential_qps": rep["qps"] / max(seq["qps"], 1e-9), "graph_gen_s": t_gen,
            "p50_us": rep["p50_us"], "p99_us": rep["p99_us"]}
     if autotune:
