@@ -1,4 +1,5 @@
-"""Learned schedule policy: graph features -> MLP -> (delta, fusion, push/pull).
+"""Learned schedule policy: graph features -> MLP -> (delta, fusion threshold,
+push/pull switch point).
 
 No counterpart in the reference, which picks delta with the Near-Far rule
 (Charlotte_oneshot/sssp_hip.cpp:59-81, hip_adds_sssp.cpp:1080-1127); that rule
@@ -6,18 +7,23 @@ stays the fallback whenever no policy is active.
 
 The MLP (24 -> 64 -> 64 -> 3, ReLU, BF16 weights with FP32 accumulation) and
 its training run in the library's own CUDA kernels (b2_policy_* in
-include/b200sssp.h).  This module adds:
+include/b200sssp.h).  Its three outputs are base-2 logarithms: the delta
+multiplier (x the Near-Far delta), the bucket-fusion threshold (frontier
+entries under which one block runs the sub-phases; off below 2^7) and the
+push/pull switch point of the heavy pass (pull when the bucket's heavy
+out-edges exceed 2^y x n; push only above 2^7).  This module adds:
 
 * ``Policy``: create / forward / gradient / train / activate;
 * weight files: ``.npz`` with ``format_version`` (``save_weights`` /
   ``load_weights``, pure numpy);
-* the label generator: a sweep of 16 log-spaced delta multipliers x fusion
-  on/off x heavy pass push-only / push-or-pull (the default switch point)
-  with the delta-stepping kernel, timed on the device, whose fastest
-  configuration is the training target;
-* ``train_default``: builds a set of synthetic graphs (ER, RMAT, perturbed
-  grids; uniform and lognormal weights), labels them, trains, and writes
-  ``policy_weights.npz`` next to this file.
+* the label generator: a sweep of 16 log-spaced delta multipliers x 4
+  fusion thresholds x 4 switch points with the delta-stepping kernel, timed
+  on the device; the label is the fastest configuration where the time is
+  flat (``robust_label``);
+* dataset building over the synthetic training family (ER, RMAT with a in
+  [0.45, 0.6], perturbed grids; 2^14 - 2^22 vertices; degree 4 - 32; uniform
+  or lognormal weights), cross-validated training, and ``compare`` (learned
+  vs fixed schedule on one graph, distances checked word for word).
 """
 from __future__ import annotations
 
@@ -34,19 +40,34 @@ from ._lib import check, lib
 N_FEATURES = 24
 N_OUTPUTS = 3
 N_PARAMS = 5955
-FORMAT_VERSION = 2   # 2: third output is the push/pull switch
+FORMAT_VERSION = 3   # 3: outputs are log2 (delta multiplier, fusion threshold, push/pull switch point)
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "policy_weights.npz")
 FEATURE_NAMES = [
     "log2_n", "log2_m", "avg_degree", "log2_1p_max_degree",
     "deg_q25", "deg_q50", "deg_q75", "deg_q90", "deg_q99", "zero_degree_frac",
     "w_q10", "w_q25", "w_q50", "w_q75", "w_q90", "log2_mean_w", "w_cv", "log2_1p_hop_depth",
     "log2_nearfar_delta", "light_frac", "is_float", "depth_capped", "w_q99", "log2_1p_avg_degree"]
-OUTPUT_NAMES = ["log2_delta_mult", "fusion_logit", "pull_logit"]
-PULL_ON = 8.0     # pull_fraction when the pull output is on (the library default)
+OUTPUT_NAMES = ["log2_delta_mult", "log2_fusion_threshold", "log2_pull_fraction"]
 # delta multipliers of the label sweep: 2^(k/2), k = -5 .. 10 (16 log-spaced values)
 SWEEP_LOG2 = [k / 2.0 for k in range(-5, 11)]
+# fusion thresholds of the sweep (log2 frontier entries; 6 stands for "off")
+FUSION_LOG2 = [6.0, 8.0, 10.0, 12.0]
+# push/pull switch points of the sweep (log2 pull_fraction; 8 stands for "push only")
+PULL_LOG2 = [1.0, 3.0, 5.0, 8.0]
 LOG2_MULT_RANGE = (-4.0, 6.0)     # the library clamps y0 to this range
-FUSION_ON = 1024
+FUSION_OFF_BELOW, FUSION_LOG2_MAX = 7.0, 14.0    # decoding of y1 (b2_policy.cu)
+PULL_OFF_ABOVE, PULL_LOG2_MIN = 7.0, 0.0         # decoding of y2
+FIXED_CONFIG = (0.0, 6.0, 3.0)    # Near-Far delta, fusion off, switch point 8 (the library defaults)
+
+
+def decode(y, dead_zone: float = 0.0) -> dict:
+    """The schedule an output vector selects (the library's rule, b2_policy.cu)."""
+    lm = float(np.clip(y[0], *LOG2_MULT_RANGE))
+    if abs(lm) < dead_zone:
+        lm = 0.0
+    fusion = 0 if y[1] < FUSION_OFF_BELOW else int(round(2.0 ** min(float(y[1]), FUSION_LOG2_MAX)))
+    pull = 0.0 if y[2] > PULL_OFF_ABOVE else float(2.0 ** max(float(y[2]), PULL_LOG2_MIN))
+    return {"delta_mult": float(2.0 ** lm), "fusion_threshold": fusion, "pull_fraction": pull}
 
 
 def _fp(a: np.ndarray):
@@ -155,11 +176,7 @@ class Policy:
 
     def decide(self, features) -> dict:
         y = self.forward(np.asarray(features, np.float32).reshape(1, -1))[0]
-        lm = float(np.clip(y[0], *LOG2_MULT_RANGE))
-        if abs(lm) < getattr(self, "dead_zone", 0.0):
-            lm = 0.0
-        return {"delta_mult": float(2.0 ** lm), "fusion": bool(y[1] > 0),
-                "pull": bool(y[2] > 0)}
+        return decode(y, getattr(self, "dead_zone", 0.0))
 
     def close(self) -> None:
         if self._h:
@@ -193,11 +210,12 @@ def activate_default(path: str = DEFAULT_WEIGHTS) -> Policy:
 
 # ---- label generation ------------------------------------------------------
 def sweep(g, sources, method: str = "delta", reps: int = 1) -> dict:
-    """Time the schedule grid on g; returns {(log2_mult, fusion, pull): ms}.
+    """Time the schedule grid on g; returns {(log2_mult, log2_fusion, log2_pull): ms}.
 
     Device time of the persistent launches (stats.kernel_ms) summed over the
-    sources; one untimed warm-up solve per configuration.  For integer weights
-    multipliers that floor to the same delta are timed once.
+    sources.  Configurations the library runs identically are timed once:
+    integer-weight multipliers that floor to the same delta, and switch points
+    whose pull can never start on g (it needs m >= pull_fraction x n).
     """
     torch = __import__("torch")
     nf = g.delta_heuristic()
@@ -208,32 +226,31 @@ def sweep(g, sources, method: str = "delta", reps: int = 1) -> dict:
         delta = nf * 2.0 ** lm
         if g.weight == "u32":
             delta = max(1.0, math.floor(delta))
-        for fu in (0, 1):
-            for lh in (0, 1):
-                key = (delta, fu, lh)
+        for fl in FUSION_LOG2:
+            fusion = 0 if fl < FUSION_OFF_BELOW else int(2 ** fl)
+            for pl in PULL_LOG2:
+                pull = 0.0 if pl > PULL_OFF_ABOVE else 2.0 ** pl
+                if pull and g.m < pull * g.n:
+                    pull = 0.0
+                key = (delta, fusion, pull)
                 if key in seen:
-                    out[(lm, fu, lh)] = seen[key]
+                    out[(lm, fl, pl)] = seen[key]
                     continue
-                kw = dict(delta=delta, fusion_threshold=FUSION_ON if fu else 0, pull_fraction=PULL_ON if lh else 0.0)
-                g.sssp(int(sources[0]), method=method, out=dist, **kw)
+                kw = dict(delta=delta, fusion_threshold=fusion, pull_fraction=pull)
                 ms = 0.0
                 for _ in range(reps):
                     for s in sources:
                         _, _, st = g.sssp(int(s), method=method, out=dist, **kw)
                         ms += st["kernel_ms"]
                 seen[key] = ms
-                out[(lm, fu, lh)] = ms
+                out[(lm, fl, pl)] = ms
     return out
 
 
 def label_from_sweep(times: dict, tol: float = 0.03):
-    """Target (log2 mult, fusion, pull) of the fastest configuration; among
-    configurations within `tol` of the best the one nearest the Near-Far delta
-    wins (labels stay stable under timing noise)."""
-    best = min(times.values())
-    near = [k for k, v in times.items() if v <= best * (1.0 + tol)]
-    k = min(near, key=lambda c: (abs(c[0]), c[1], -c[2]))
-    return np.array([k[0], float(k[1]), float(k[2])], np.float32), best
+    """Target (log2 mult, log2 fusion, log2 pull) of one sweep and the best time."""
+    A = times_array(times)
+    return robust_label(A, tol), float(A.min())
 
 
 # ---- synthetic training graphs ----------------------------------------------
@@ -249,7 +266,7 @@ def _weights(rng, m, kind, wtype):
     return (w / w.max()).astype(np.float32)
 
 
-def training_graph(i: int, max_scale: int = 23, min_scale: int = 16):
+def training_graph(i: int, max_scale: int = 22, min_scale: int = 14):
     """Deterministic graph #i of the training family (host arrays): ER, RMAT
     (a in [0.45, 0.6]) and perturbed grids; 2^min_scale .. 2^max_scale
     vertices; uniform or lognormal weights, uint32 or float."""
@@ -278,41 +295,54 @@ def training_graph(i: int, max_scale: int = 23, min_scale: int = 16):
 
 
 def times_array(times: dict) -> np.ndarray:
-    """Sweep dict -> [16 multipliers, fusion, pull] array of ms."""
-    A = np.zeros((len(SWEEP_LOG2), 2, 2))
-    for (lm, fu, lh), v in times.items():
-        A[SWEEP_LOG2.index(lm), fu, lh] = v
+    """Sweep dict -> [16 multipliers, 4 fusion thresholds, 4 switch points] array of ms."""
+    A = np.zeros((len(SWEEP_LOG2), len(FUSION_LOG2), len(PULL_LOG2)))
+    for (lm, fl, pl), v in times.items():
+        A[SWEEP_LOG2.index(lm), FUSION_LOG2.index(fl), PULL_LOG2.index(pl)] = v
     return A
 
 
-def build_dataset(count: int, max_scale: int = 23, n_sources: int = 3, min_scale: int = 16, log=print,
-                  first: int = 0, checkpoint: str | None = None):
+def build_dataset(count: int, max_scale: int = 22, n_sources: int = 2, min_scale: int = 14, log=print,
+                  first: int = 0, checkpoint: str | None = None, every: int = 10):
     """Features X, labels T, full sweep tables and descriptions of graphs
-    first .. first + count - 1 of the training family.  With `checkpoint`
-    the partial dataset is saved after every graph."""
+    first .. first + count - 1 of the training family.  The next graph is
+    generated on a host thread while the current one is swept.  With
+    `checkpoint` the partial dataset is saved every `every` graphs."""
+    from concurrent.futures import ThreadPoolExecutor
     from . import Graph
     X, T, TT, info = [], [], [], []
-    for i in range(first, first + count):
-        hg, w, wtype, desc = training_graph(i, max_scale, min_scale)
-        g = Graph.from_arrays(hg.rowptr, hg.colind, w, weight=wtype)
-        rng = np.random.default_rng(i)
-        cand = np.nonzero(np.diff(hg.rowptr) > 0)[0]        # sources with out-edges
-        srcs = rng.choice(cand, size=min(n_sources, cand.size), replace=False) if cand.size else [0]
-        del hg, w, cand
-        t0 = time.time()
-        X.append(graph_features(g))
-        times = sweep(g, srcs)
-        y, best = label_from_sweep(times)
-        base = times[(0.0, 0, 1)]
-        T.append(y)
-        TT.append(times_array(times))
-        desc.update(index=i, best_ms=best, fixed_ms=base, gain=base / best, label=y.tolist())
-        info.append(desc)
-        log(f"[{i}] {desc} sweep {time.time() - t0:.1f}s")
-        g.close()
-        if checkpoint:
-            save_dataset(checkpoint, np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info)
+    with ThreadPoolExecutor(max_workers=1) as ex:
+        nxt = ex.submit(training_graph, first, max_scale, min_scale)
+        for i in range(first, first + count):
+            hg, w, wtype, desc = nxt.result()
+            if i + 1 < first + count:
+                nxt = ex.submit(training_graph, i + 1, max_scale, min_scale)
+            g = Graph.from_arrays(hg.rowptr, hg.colind, w, weight=wtype)
+            rng = np.random.default_rng(i)
+            cand = np.nonzero(np.diff(hg.rowptr) > 0)[0]        # sources with out-edges
+            srcs = rng.choice(cand, size=min(n_sources, cand.size), replace=False) if cand.size else [0]
+            del hg, w, cand
+            t0 = time.time()
+            X.append(graph_features(g))
+            times = sweep(g, srcs)
+            y, best = label_from_sweep(times)
+            base = times[FIXED_CONFIG]
+            T.append(y)
+            TT.append(times_array(times))
+            desc.update(index=i, best_ms=best, fixed_ms=base, gain=base / best, label=y.tolist())
+            info.append(desc)
+            log(f"[{i}] {desc} sweep {time.time() - t0:.1f}s")
+            g.close()
+            if checkpoint and (len(X) % every == 0 or i + 1 == first + count):
+                save_dataset(checkpoint, np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info)
     return np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info
+
+
+def merge_datasets(paths, out: str) -> None:
+    """Concatenate saved sweep datasets (in the order given)."""
+    parts = [load_dataset(p) for p in paths]
+    save_dataset(out, np.concatenate([q[0] for q in parts]), np.concatenate([q[1] for q in parts]),
+                 np.concatenate([q[2] for q in parts]), [d for q in parts for d in q[3]])
 
 
 def save_dataset(path: str, X, T, TT, info) -> None:
@@ -337,7 +367,7 @@ def train_on(X, T, epochs: int = 3000, lr: float = 3e-3, weight_decay: float = 1
     return p
 
 
-def train_default(count: int = 200, max_scale: int = 23, epochs: int = 3000, lr: float = 3e-3,
+def train_default(count: int = 200, max_scale: int = 22, epochs: int = 3000, lr: float = 3e-3,
                   weight_decay: float = 1e-3, out: str = DEFAULT_WEIGHTS, dataset_out: str | None = None,
                   log=print):
     X, T, TT, info = build_dataset(count, max_scale, log=log)
@@ -349,39 +379,52 @@ def train_default(count: int = 200, max_scale: int = 23, epochs: int = 3000, lr:
 
 
 # ---- robust labels, decision cost, cross-validated training ---------------
-FIXED_INDEX = (SWEEP_LOG2.index(0.0), 0, 1)   # Near-Far delta, no fusion, default push/pull switch
+FIXED_INDEX = (SWEEP_LOG2.index(FIXED_CONFIG[0]), FUSION_LOG2.index(FIXED_CONFIG[1]),
+               PULL_LOG2.index(FIXED_CONFIG[2]))
 
 
 def robust_label(A: np.ndarray, tol: float = 0.03) -> np.ndarray:
-    """Label of one sweep table A[16 multipliers, fusion, pull] (ms).
+    """Label of one sweep table A[16 multipliers, 4 fusion, 4 switch points] (ms).
 
     Each configuration is scored by its worst time over itself and its two
-    neighbouring multipliers (x 2^-0.5, x 2^0.5) at the same fusion / split
+    neighbouring multipliers (x 2^-0.5, x 2^0.5) at the same fusion / switch
     setting, so a label sits where the time is flat and a prediction that
     misses by half a step in log2 costs little.  Among scores within `tol` of
-    the best, the multiplier nearest 1 wins (then fusion off, pull allowed)."""
+    the best, the multiplier nearest 1 wins, then the library's default fusion
+    and switch point.  Returns (log2 mult, log2 fusion, log2 switch point)."""
     L = A.shape[0]
     score = np.empty_like(A)
     for i in range(L):
         lo, hi = max(0, i - 1), min(L - 1, i + 1)
         score[i] = A[lo:hi + 1].max(axis=0)
     best = score.min()
-    cand = [(abs(SWEEP_LOG2[i]), f, -h, i) for i in range(L) for f in (0, 1) for h in (0, 1)
-            if score[i, f, h] <= best * (1.0 + tol)]
-    _, f, nh, i = min(cand)
-    return np.array([SWEEP_LOG2[i], float(f), float(-nh)], np.float32)
+    f0, p0 = FIXED_INDEX[1], FIXED_INDEX[2]
+    cand = [(abs(SWEEP_LOG2[i]), f != f0, p != p0, abs(f - f0) + abs(p - p0), i, f, p)
+            for i in range(L) for f in range(A.shape[1]) for p in range(A.shape[2])
+            if score[i, f, p] <= best * (1.0 + tol)]
+    *_, i, f, p = min(cand)
+    return np.array([SWEEP_LOG2[i], FUSION_LOG2[f], PULL_LOG2[p]], np.float32)
 
 
 def decision_index(y, dead_zone: float = 0.0) -> tuple[int, int, int]:
-    """Sweep-grid configuration nearest to an MLP output (log2 mult, fusion
-    logit, pull logit), with the library's clamp of the multiplier.  A
-    predicted |log2 multiplier| under `dead_zone` keeps the Near-Far delta
-    (the library applies the same rule, b2_policy_set_dead_zone)."""
+    """Sweep-grid configuration nearest to the schedule an MLP output selects
+    (the library's decoding: clamped multiplier and dead zone, fusion off below
+    2^7, push only above 2^7)."""
     lm = float(np.clip(y[0], *LOG2_MULT_RANGE))
     if abs(lm) < dead_zone:
         lm = 0.0
     i = int(np.argmin([abs(lm - v) for v in SWEEP_LOG2]))
-    return i, int(y[1] > 0), int(y[2] > 0)
+    if y[1] < FUSION_OFF_BELOW:
+        f = 0
+    else:
+        fl = min(float(y[1]), FUSION_LOG2_MAX)
+        f = 1 + int(np.argmin([abs(fl - v) for v in FUSION_LOG2[1:]]))
+    if y[2] > PULL_OFF_ABOVE:
+        p = len(PULL_LOG2) - 1
+    else:
+        pl = max(float(y[2]), PULL_LOG2_MIN)
+        p = int(np.argmin([abs(pl - v) for v in PULL_LOG2[:-1]]))
+    return i, f, p
 
 
 def decision_speedup(A: np.ndarray, y, dead_zone: float = 0.0) -> float:
@@ -485,16 +528,24 @@ def compare(g, sources, method: str = "delta", reps: int = 3) -> dict:
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser(description="label synthetic graphs by schedule sweeps and train the policy")
-    ap.add_argument("--graphs", type=int, default=200)
-    ap.add_argument("--max-scale", type=int, default=23)
-    ap.add_argument("--epochs", type=int, default=3000)
-    ap.add_argument("--weight-decay", type=float, default=1e-3)
+    ap.add_argument("--graphs", type=int, default=2000)
+    ap.add_argument("--first", type=int, default=0, help="index of the first training graph to sweep")
+    ap.add_argument("--min-scale", type=int, default=14)
+    ap.add_argument("--max-scale", type=int, default=22)
+    ap.add_argument("--checkpoint", default=None, help="sweep only: save the partial dataset here")
+    ap.add_argument("--merge", nargs="+", default=None, help="concatenate these sweep datasets into --dataset-out")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--dataset-out", default=None)
-    ap.add_argument("--from-dataset", default=None, help="retrain from a saved sweep dataset (cross-validated)")
+    ap.add_argument("--from-dataset", default=None, help="train from a saved sweep dataset (cross-validated)")
     a = ap.parse_args()
-    if a.from_dataset:
+    if a.merge:
+        merge_datasets(a.merge, a.dataset_out)
+    elif a.from_dataset:
         train_from_dataset(a.from_dataset, out=a.out)
+    elif a.checkpoint:
+        build_dataset(a.graphs, a.max_scale, min_scale=a.min_scale, first=a.first, checkpoint=a.checkpoint)
     else:
-        train_default(a.graphs, a.max_scale, a.epochs, weight_decay=a.weight_decay, out=a.out,
-                      dataset_out=a.dataset_out)
+        X, T, TT, info = build_dataset(a.graphs, a.max_scale, min_scale=a.min_scale, first=a.first)
+        if a.dataset_out:
+            save_dataset(a.dataset_out, X, T, TT, info)
+        train_on(X, T, out=a.out, max_scale=np.int32(a.max_scale))

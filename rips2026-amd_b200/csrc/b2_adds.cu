@@ -878,8 +878,9 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   double delta = o.delta;
   if (o.policy == 1) {
     double mult = 1.0;
-    int32_t fuse = 0, pull = 1;
-    const b2_status ps = policy_decide(g, &mult, &fuse, &pull);
+    uint32_t fuse = 0;
+    float pull = 8.0f;
+    const b2_status ps = policy_decide(g, &mult, &fuse, &pull);   // ADDS takes the width only
     if (ps == B2_SUCCESS) {
       double nf = 1.0;
       b2_delta_heuristic(g, o.delta_scale > 0 ? o.delta_scale : 16.0, &nf);

@@ -291,8 +291,8 @@ struct b2_graph_s {
   bool features_valid = false;
   uint64_t pol_version = 0;     // policy decision cache: valid when equal to the
   double pol_mult = 1.0;        // active policy's version
-  int32_t pol_fusion = 0;
-  int32_t pol_pull = 1;
+  uint32_t pol_fusion = 0;      // bucket-fusion threshold (0: off)
+  float pol_pull = 8.0f;        // push/pull switch point (0: push only)
   b2::Workspace ws;
   std::mutex mu;   // one solve at a time per handle
 };
@@ -315,9 +315,10 @@ b2_status collect_reach(b2_graph g, const void* labels, bool pred, bool isf, cud
 b2_status ensure_incoming(b2_graph g, cudaStream_t st);
 // Internal id of input vertex `v` (identity unless the graph is in degree order).
 inline uint32_t internal_id(b2_graph g, uint32_t v) { return g->inv_host.empty() ? v : g->inv_host[v]; }
-// Learned schedule: delta multiplier (x Near-Far delta), fusion and push/pull
-// choice for g.  B2_NOT_SUPPORTED when no policy is active.
-b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* pull_on);
+// Learned schedule: delta multiplier (x Near-Far delta), bucket-fusion
+// threshold (0: off) and push/pull switch point (pull_fraction; 0: push only)
+// for g.  B2_NOT_SUPPORTED when no policy is active.
+b2_status policy_decide(b2_graph g, double* delta_mult, uint32_t* fusion_threshold, float* pull_fraction);
 b2_status graph_from_device_outgoing(int64_t n, int64_t m, const uint64_t* rowptr, const uint2* edges,
                                      int weight_type, b2_graph* out);
 }  // namespace b2

@@ -1,5 +1,6 @@
-// Learned schedule policy: graph features -> MLP 24 -> 64 -> 64 -> 3 -> (delta
-// multiplier, bucket fusion on/off, push/pull switch of the heavy pass).
+// Learned schedule policy: graph features -> MLP 24 -> 64 -> 64 -> 3 -> (log2
+// delta multiplier, log2 bucket-fusion threshold, log2 push/pull switch point
+// of the heavy pass).
 //
 // No reference counterpart (the reference picks delta with the Near-Far rule,
 // Charlotte_oneshot/sssp_hip.cpp:59-81, and adapts it in hip_adds).  The
@@ -11,7 +12,13 @@
 // FP32.  Forward/backward run one 64-thread block per sample; per-sample
 // gradients are written to a [batch x params] buffer and summed in a fixed
 // order by a second kernel, so a training step is deterministic.
-// Loss per sample: (y0 - t0)^2 + BCE(y1, t1) + BCE(y2, t2) (BCE on logits).
+// Loss per sample: sum over the three outputs of (y - t)^2 (every output is a
+// base-2 logarithm, so the loss weighs relative errors).
+// Decoding (policy_decide): delta = Near-Far delta x 2^clamp(y0, -4, 6)
+// (|y0| under the dead zone keeps the Near-Far delta); fusion threshold =
+// 2^clamp(y1, 7, 14) frontier entries, off when y1 < 7; the heavy pass may
+// pull when the bucket's heavy out-edges exceed 2^clamp(y2, 0, 7) x n, push
+// only when y2 > 7.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -67,7 +74,6 @@ __global__ void k_mlp_forward(const __nv_bfloat16* __restrict__ w, const float* 
   }
 }
 
-__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf(-z)); }
 
 // per-sample loss and gradient of the mean loss (divided by B) -> G[s * kParams ...]
 __global__ void k_mlp_backward(const __nv_bfloat16* __restrict__ w, const float* __restrict__ X,
@@ -80,15 +86,12 @@ __global__ void k_mlp_backward(const __nv_bfloat16* __restrict__ w, const float*
     __syncthreads();
     mlp_forward(w, x, h1, h2, y);
     if (j == 0) {
-      const float t0 = T[s * kOut + 0], t1 = T[s * kOut + 1], t2 = T[s * kOut + 2];
-      const float e0 = y[0] - t0;
-      float loss = e0 * e0;
-      dy[0] = 2.0f * e0 * inv_b;
-      const float z1 = y[1], z2 = y[2];
-      loss += fmaxf(z1, 0.0f) - z1 * t1 + log1pf(expf(-fabsf(z1)));
-      loss += fmaxf(z2, 0.0f) - z2 * t2 + log1pf(expf(-fabsf(z2)));
-      dy[1] = (sigmoidf_(z1) - t1) * inv_b;
-      dy[2] = (sigmoidf_(z2) - t2) * inv_b;
+      float loss = 0.0f;
+      for (int k = 0; k < kOut; ++k) {
+        const float e = y[k] - T[s * kOut + k];
+        loss = fmaf(e, e, loss);
+        dy[k] = 2.0f * e * inv_b;
+      }
       L[s] = loss;
     }
     __syncthreads();
@@ -209,6 +212,8 @@ void normalize(const b2_policy p, const float* raw, float* out, int B) {
 
 constexpr int kSample = 65536;
 constexpr double kLog2MultMin = -4.0, kLog2MultMax = 6.0;   // clamp of output y0
+constexpr double kFusionOffBelow = 7.0, kFusionLog2Max = 14.0;   // output y1
+constexpr double kPullOffAbove = 7.0, kPullLog2Min = 0.0;       // output y2
 constexpr int kDepthCap = 256;   // hop-depth probe: at most this many Bellman-Ford rounds
 
 // The 24 features: size (log n, log m, m/n, log max degree), out-degree
@@ -308,7 +313,7 @@ b2_status run_forward(b2_policy p, const float* xn_host, int B, float* y_host) {
 }
 }  // namespace
 
-b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int32_t* pull_on) {
+b2_status policy_decide(b2_graph g, double* delta_mult, uint32_t* fusion_threshold, float* pull_fraction) {
   std::lock_guard<std::mutex> lock(g_pol_mu);
   if (!g_active) return B2_NOT_SUPPORTED;
   if (g->pol_version != g_generation) {
@@ -321,13 +326,16 @@ b2_status policy_decide(b2_graph g, double* delta_mult, int32_t* fusion_on, int3
     double lm = std::max(kLog2MultMin, std::min(kLog2MultMax, (double)y[0]));
     if (std::fabs(lm) < (double)g_active->s.dead_zone) lm = 0.0;
     g->pol_mult = std::exp2(lm);
-    g->pol_fusion = y[1] > 0.0f ? 1 : 0;
-    g->pol_pull = y[2] > 0.0f ? 1 : 0;
+    g->pol_fusion = (double)y[1] < kFusionOffBelow
+                        ? 0u
+                        : (uint32_t)std::lround(std::exp2(std::min(kFusionLog2Max, (double)y[1])));
+    g->pol_pull = (double)y[2] > kPullOffAbove ? 0.0f
+                                               : (float)std::exp2(std::max(kPullLog2Min, (double)y[2]));
     g->pol_version = g_generation;
   }
   *delta_mult = g->pol_mult;
-  *fusion_on = g->pol_fusion;
-  *pull_on = g->pol_pull;
+  *fusion_threshold = g->pol_fusion;
+  *pull_fraction = g->pol_pull;
   return B2_SUCCESS;
 }
 

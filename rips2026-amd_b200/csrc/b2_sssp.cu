@@ -45,6 +45,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -111,6 +112,7 @@ struct Params {
   uint32_t dense_min;     // delta: near / slot frontiers of at least this many entries are swept
   uint32_t qcap;          // entries each worklist queue may hold (<= n; a push past it is kErrQueueOverflow)
   ProgressBoard* board;   // mapped progress record (null: no progress callback)
+  uint32_t small_items;   // queue items shrink below 32 vertices for small frontiers
 };
 
 // Bucket of a distance key under the phase's mapping
@@ -578,22 +580,22 @@ __device__ __forceinline__ uint32_t sweep_span(const Params& P, const PhaseRec& 
   return carry + total;
 }
 
-// One frontier work item: entries [32 item, 32 item + 32) of the frontier
-// queue, or the frontier vertices of sweep span `item`.  A sweep expands only
-// whole groups of 32 and carries the rest (`carry`) into the warp's next
-// item, so sparse spans do not run lanes idle; `flush` expands the carried
-// rest at the end of the phase.
+// One frontier work item: entries [g item, g item + g) of the frontier queue
+// (g <= 32 vertices, one per lane), or the frontier vertices of sweep span
+// `item`.  A sweep expands only whole groups of 32 and carries the rest
+// (`carry`) into the warp's next item, so sparse spans do not run lanes idle;
+// `flush` expands the carried rest at the end of the phase.
 template <class W, bool PRED, int MODE>
 __device__ __forceinline__ void frontier_item(const Params& P, const PhaseRec& R, uint32_t item, bool dense,
-                                              bool flush, uint32_t& carry, Tally& t) {
+                                              bool flush, uint32_t& carry, Tally& t, uint32_t g = 32) {
   const uint32_t lane = lane_id();
-  const uint32_t base = item * 32;
+  const uint32_t base = item * g;
   uint32_t total, limit;
   if (dense) {
     total = flush ? carry : sweep_span(P, R, item, t.q.listb, carry);
     limit = flush ? total : (total & ~31u);
   } else {
-    total = min(32u, R.fcount - base);
+    total = min(g, R.fcount - base);
     limit = total;
   }
   for (uint32_t j0 = 0; j0 < limit; j0 += 32) {
@@ -629,15 +631,24 @@ constexpr uint32_t kHubGrab = B2_HUB_GRAB;   // hub chunks per work item
 // round-robin to the warps (3/4 of them, no atomics), the rest handed out one
 // at a time from a phase counter so no warp idles while another holds a long
 // tail.
+//
+// Queue items hold g vertices: 32 when the frontier gives every warp at least
+// one full item, else the largest power of two that still does, down to one
+// vertex per warp.  A small frontier of long rows (a few hundred vertices of
+// ~200 edges) then spreads over the grid instead of leaving a few warps to
+// walk 32 long rows each while the rest wait at the barrier.
 template <class W, bool PRED, int MODE>
 __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t nhub = min(R.hub_in_chunks, P.hub_cap);
   const uint32_t nhg = (nhub + kHubGrab - 1) / kHubGrab;
   const bool dense = MODE == kModeDelta && R.dense != kDenseOff;
-  const uint32_t nfc = dense ? (P.n + kDenseSpan - 1) / kDenseSpan : (R.fcount + 31) / 32;
-  const uint32_t items = nhg + nfc;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t g = 32;
+  if (!dense && P.small_items)
+    while (g > 1 && (R.fcount + g - 1) / g < nwarps) g >>= 1;
+  const uint32_t nfc = dense ? (P.n + kDenseSpan - 1) / kDenseSpan : (R.fcount + g - 1) / g;
+  const uint32_t items = nhg + nfc;
   const uint32_t rounds = (items * B2_STATIC_NUM / 4) / nwarps;
   const uint32_t nstatic = rounds * nwarps;
   Control* c = P.ctl;
@@ -656,7 +667,7 @@ __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
       const uint32_t h1 = min(nhub, (item + 1) * kHubGrab);
       for (uint32_t h = item * kHubGrab; h < h1; ++h) hub_chunk<W, PRED, MODE>(P, R, h, t);
     } else {
-      frontier_item<W, PRED, MODE>(P, R, done ? 0u : item - nhg, dense, done, carry, t);
+      frontier_item<W, PRED, MODE>(P, R, done ? 0u : item - nhg, dense, done, carry, t, g);
     }
     if (done) break;
   }
@@ -1480,16 +1491,16 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     // learned schedule (computes and caches the graph's features on first use,
     // which runs solves of its own: before this solve takes the handle lock)
     double mult = 1.0;
-    int32_t fuse = 0, pull = 1;
+    uint32_t fuse = 0;
+    float pull = 8.0f;
     const b2_status ps = policy_decide(g, &mult, &fuse, &pull);
     if (ps == B2_SUCCESS) {
       double nf = 1.0;
       b2_delta_heuristic(g, o.delta_scale > 0 ? o.delta_scale : 16.0, &nf);
       o.delta = nf * mult;
-      if (o.fusion_threshold == 0) o.fusion_threshold = fuse ? 1024u : 0u;
-      // push/pull switch of the heavy pass: the default switch point, or push only
+      if (o.fusion_threshold == 0) o.fusion_threshold = fuse;
       o.light_heavy = 1;
-      o.pull_fraction = pull ? (o.pull_fraction > 0.0f ? o.pull_fraction : 8.0f) : 0.0f;
+      o.pull_fraction = pull;   // the predicted push/pull switch point (0: push only)
       policy_used = 1;
     } else if (ps != B2_NOT_SUPPORTED) {
       return ps;
@@ -1504,6 +1515,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   memset(&P, 0, sizeof(P));
   P.n = (uint32_t)g->n;
   P.qcap = (o.worklist_capacity > 0 && (int64_t)o.worklist_capacity < g->n) ? o.worklist_capacity : P.n;
+  P.small_items = std::getenv("B2_ITEM32") ? 0u : 1u;
   P.source = internal_id(g, source);
   P.perm = g->perm;
   P.inv = g->perm ? g->inv : nullptr;

@@ -32,7 +32,7 @@ def test_gradient_matches_fp64_oracle(pol, orc):
     p = pol.Policy(seed=5)
     rng = np.random.default_rng(1)
     X = rng.normal(size=(50, 24)).astype(np.float32)
-    T = np.c_[rng.normal(size=50), rng.integers(0, 2, (50, 2))].astype(np.float32)
+    T = np.c_[rng.normal(size=50), rng.uniform(6, 12, 50), rng.uniform(1, 8, 50)].astype(np.float32)
     # non-trivial normalization
     P, _, _ = p.params()
     mu = rng.normal(size=24).astype(np.float32)
@@ -51,7 +51,8 @@ def test_training_is_deterministic_and_fits(pol):
     rng = np.random.default_rng(2)
     X = rng.normal(size=(64, 24)).astype(np.float32)
     w = rng.normal(size=24)
-    T = np.c_[np.tanh(X @ w / 5) * 3, (X[:, 0] > 0), (X[:, 1] < 0)].astype(np.float32)
+    T = np.c_[np.tanh(X @ w / 5) * 3, np.where(X[:, 0] > 0, 10.0, 6.0), np.where(X[:, 1] < 0, 8.0, 3.0)]
+    T = T.astype(np.float32)
     a, b = pol.Policy(seed=3), pol.Policy(seed=3)
     la = a.train(X, T, epochs=600, lr=3e-3)
     lb = b.train(X, T, epochs=600, lr=3e-3)
@@ -60,7 +61,7 @@ def test_training_is_deterministic_and_fits(pol):
     _, l0 = pol.Policy(seed=3).gradient(X, T)
     assert la < 0.25 * l0
     Y = a.forward(X)
-    assert ((Y[:, 1] > 0) == (T[:, 1] > 0.5)).mean() > 0.9
+    assert ((Y[:, 1] > 8.0) == (T[:, 1] > 8.0)).mean() > 0.9
 
 
 def _raw(d, weight):
@@ -83,14 +84,14 @@ def test_policy_sets_schedule_and_keeps_distances(pol, b2, orc, cuda, weight):
     w = hg.weights if weight == "u32" else hg.fweights
     ref = orc.dijkstra(hg.rowptr, hg.colind, w, 3)
     p = pol.Policy()
-    _set_constant(p, [2.0, -1.0, 1.0])            # delta x4, fusion off, pull allowed
+    _set_constant(p, [2.0, 6.0, 3.0])             # delta x4, fusion off, pull past 8 n heavy edges
     p.activate()
     d, _, st = g.sssp(3, policy=1)
     assert st["policy_used"] == 1
     want = max(1.0, np.floor(nf * 4.0)) if weight == "u32" else nf * 4.0
     assert st["delta_used"] == pytest.approx(want, rel=1e-12)
     assert np.array_equal(_raw(d, weight), ref)
-    _set_constant(p, [-9.0, 1.0, -1.0])            # clamped to /16, fusion on, push only
+    _set_constant(p, [-9.0, 10.0, 7.5])            # clamped to /16, fusion threshold 1024, push only
     d2, _, st2 = g.sssp(3, policy=1, trace=1)
     assert st2["policy_used"] == 1
     want = max(1.0, np.floor(nf / 16.0)) if weight == "u32" else nf / 16.0
@@ -138,7 +139,7 @@ def test_dead_zone_keeps_near_far_delta(pol, b2, cuda):
     g = b2.Graph.from_host(hg, "f32")
     nf = g.delta_heuristic()
     p = pol.Policy()
-    _set_constant(p, [0.375, -1.0, 1.0])            # (exact in bfloat16)
+    _set_constant(p, [0.375, 6.0, 3.0])             # (exact in bfloat16)
     p.set_dead_zone(0.5)
     p.activate()
     _, _, st = g.sssp(0, policy=1)

@@ -10,7 +10,7 @@ def test_oracle_gradient_matches_finite_differences(orc):
     rng = np.random.default_rng(3)
     P = rng.normal(0, 0.2, 5955)
     X = rng.normal(size=(9, 24))
-    T = np.c_[rng.normal(size=9), rng.integers(0, 2, (9, 2))]
+    T = np.c_[rng.normal(size=9), rng.uniform(6, 12, 9), rng.uniform(1, 8, 9)]
     _, g = orc.mlp_loss_grad(P, X, T)
     eps = 1e-6
     for i in rng.choice(5955, 60, replace=False):
@@ -60,13 +60,34 @@ def test_shipped_weights_load(b2):
 
 def test_label_rule():
     from b200sssp import policy as pol
-    times = {(lm, fu, lh): 10.0 for lm in pol.SWEEP_LOG2 for fu in (0, 1) for lh in (0, 1)}
-    times[(2.0, 1, 0)] = 5.0
-    times[(-1.0, 0, 1)] = 5.05       # within 3 %: nearer the Near-Far delta, wins
+    times = {(lm, fl, pl): 10.0 for lm in pol.SWEEP_LOG2 for fl in pol.FUSION_LOG2 for pl in pol.PULL_LOG2}
+    for lm in (1.5, 2.0, 2.5):
+        times[(lm, 10.0, 8.0)] = 5.0          # a flat optimum: x 2^2, fusion 1024, push only
+    times[(-1.0, 6.0, 3.0)] = 5.05            # a sharp dip: its neighbours are slow
     y, best = pol.label_from_sweep(times)
-    assert y.tolist() == [-1.0, 0.0, 1.0] and best == 5.0
+    assert y.tolist() == [2.0, 10.0, 8.0] and best == 5.0
+    for lm in (-1.5, -1.0, -0.5):
+        times[(lm, 6.0, 3.0)] = 5.1           # now flat too and within 3 %: nearer the Near-Far delta
+    y, _ = pol.label_from_sweep(times)
+    assert y.tolist() == [-1.0, 6.0, 3.0]
     y, _ = pol.label_from_sweep(times, tol=0.0)
-    assert y.tolist() == [2.0, 1.0, 0.0]
+    assert y.tolist() == [2.0, 10.0, 8.0]
+
+
+def test_decoding_matches_the_library_rule():
+    """Outputs are log2 values: the multiplier is clamped and has a dead zone,
+    fusion is off below 2^7, the heavy pass pushes only above 2^7."""
+    from b200sssp import policy as pol
+    d = pol.decode([0.3, 9.0, 2.0])
+    assert d == {"delta_mult": pytest.approx(2 ** 0.3), "fusion_threshold": 512, "pull_fraction": 4.0}
+    assert pol.decode([0.3, 9.0, 2.0], dead_zone=0.5)["delta_mult"] == 1.0
+    d = pol.decode([99.0, 6.9, 7.1])
+    assert d["delta_mult"] == 2.0 ** 6 and d["fusion_threshold"] == 0 and d["pull_fraction"] == 0.0
+    d = pol.decode([-99.0, 30.0, -5.0])
+    assert d["delta_mult"] == 2.0 ** -4 and d["fusion_threshold"] == 2 ** 14 and d["pull_fraction"] == 1.0
+    L = len(pol.SWEEP_LOG2)
+    assert pol.decision_index([99.0, 11.2, 2.1]) == (L - 1, 3, 1)
+    assert pol.decision_index([0.1, 6.5, 7.5]) == (pol.SWEEP_LOG2.index(0.0), 0, 3)
 
 
 def test_robust_label_prefers_flat_side():
@@ -74,21 +95,23 @@ def test_robust_label_prefers_flat_side():
     the decision cost reads the chosen configuration off the sweep table."""
     from b200sssp import policy as pol
     L = len(pol.SWEEP_LOG2)
-    A = np.full((L, 2, 2), 10.0)
+    A = np.full((L, 4, 4), 10.0)
     i0 = pol.SWEEP_LOG2.index(0.0)
-    A[:, 0, 1] = 10.0
-    A[i0 - 2, 0, 1] = 7.0          # sharp minimum at x 2^-1 ...
-    A[i0 - 3, 0, 1] = 30.0         # ... next to a cliff
-    A[i0 + 2: i0 + 5, 0, 1] = 8.0  # flat region at x 2^1 .. 2^2
+    f0, p0 = pol.FIXED_INDEX[1], pol.FIXED_INDEX[2]
+    A[i0 - 2, f0, p0] = 7.0          # sharp minimum at x 2^-1 ...
+    A[i0 - 3, f0, p0] = 30.0         # ... next to a cliff
+    A[i0 + 2: i0 + 5, f0, p0] = 8.0  # flat region at x 2^1 .. 2^2
     y = pol.robust_label(A)
-    assert y.tolist() == [1.5, 0.0, 1.0]          # middle of the flat region
+    assert y.tolist() == [1.5, 6.0, 3.0]          # middle of the flat region
     assert pol.decision_speedup(A, y) == pytest.approx(10.0 / 8.0)
-    assert pol.decision_speedup(A, [-1.0, -3.0, 2.0]) == pytest.approx(10.0 / 7.0)
-    assert pol.decision_index([99.0, 1.0, -1.0]) == (L - 1, 1, 0)   # clamped multiplier
+    assert pol.decision_speedup(A, [-1.0, 0.0, 3.2]) == pytest.approx(10.0 / 7.0)
 
 
 def test_shipped_dataset_matches_weights():
     from b200sssp import policy as pol
     X, T, TT, info = pol.load_dataset(os.path.join(os.path.dirname(pol.DEFAULT_WEIGHTS), "policy_dataset.npz"))
     assert X.shape[0] == TT.shape[0] == len(info) > 0
-    assert TT.shape[1:] == (len(pol.SWEEP_LOG2), 2, 2) and np.isfinite(TT).all()
+    assert TT.shape[1:] == (len(pol.SWEEP_LOG2), len(pol.FUSION_LOG2), len(pol.PULL_LOG2))
+    assert np.isfinite(TT).all() and (TT > 0).all()
+    w = pol.load_weights()
+    assert int(w["n_graphs"]) == X.shape[0]
