@@ -268,8 +268,12 @@ def _weights(rng, m, kind, wtype):
 
 def training_graph(i: int, max_scale: int = 22, min_scale: int = 14):
     """Deterministic graph #i of the training family (host arrays): ER, RMAT
-    (a in [0.45, 0.6]) and perturbed grids; 2^min_scale .. 2^max_scale
-    vertices; uniform or lognormal weights, uint32 or float."""
+    (a in [0.45, 0.6]) and perturbed grids (0 - 5 % random shortcuts);
+    2^min_scale .. 2^max_scale vertices, average degree 4 - 32 (4 - 16 past
+    2^20 vertices); uniform or lognormal (sigma 0.5 - 2) weights, uint32 or
+    float.  ER graphs past 2^18 vertices are drawn as RMAT with equal quadrant
+    probabilities (uniform endpoints, symmetrised), which the library
+    generates in parallel."""
     from . import gen_er, gen_grid, gen_rmat
     rng = np.random.default_rng(1000 + i)
     fam = ["er", "rmat", "grid"][i % 3]
@@ -277,19 +281,18 @@ def training_graph(i: int, max_scale: int = 22, min_scale: int = 14):
     wkind = "uniform" if rng.uniform() < 0.5 else "lognormal"
     sc = int(rng.integers(min_scale, max_scale + 1))
     deg = int(rng.choice([4, 8, 16, 32] if sc <= 20 else [4, 8, 16]))
-    if fam == "er":
+    if fam == "er" and sc <= 18:
         hg = gen_er(1 << sc, deg << sc, 1, 2, seed=i)
+    elif fam == "er":
+        hg = gen_rmat(sc, max(1, deg // 2), 0.25, 0.25, 0.25, 1, 2, seed=i)
     elif fam == "rmat":
         a = float(rng.uniform(0.45, 0.6))
         bc = (1.0 - a) / 3.0
         hg = gen_rmat(sc, deg, a, bc, bc, 1, 2, seed=i)
     else:
         side = int(2 ** rng.uniform(7, (sc + 1) / 2.0))
-        hg = gen_grid(side, side, float(rng.choice([0.0, 0.01, 0.05])), 5.0, 1.0, seed=i)
-    if fam == "grid" and wkind == "lognormal":
-        w = hg.weights if wtype == "u32" else hg.fweights     # the generator's own lognormal law
-    else:
-        w = _weights(rng, hg.m, wkind, wtype)
+        hg = gen_grid(side, side, float(rng.choice([0.0, 0.01, 0.02, 0.05])), 5.0, 1.0, seed=i)
+    w = _weights(rng, hg.m, wkind, wtype)
     desc = {"family": fam, "n": hg.n, "m": hg.m, "weights": wkind, "wtype": wtype}
     return hg, w, wtype, desc
 
@@ -303,11 +306,14 @@ def times_array(times: dict) -> np.ndarray:
 
 
 def build_dataset(count: int, max_scale: int = 22, n_sources: int = 2, min_scale: int = 14, log=print,
-                  first: int = 0, checkpoint: str | None = None, every: int = 10):
+                  first: int = 0, checkpoint: str | None = None, every: int = 10, seconds: float = 0.0):
     """Features X, labels T, full sweep tables and descriptions of graphs
     first .. first + count - 1 of the training family.  The next graph is
     generated on a host thread while the current one is swept.  With
-    `checkpoint` the partial dataset is saved every `every` graphs."""
+    `checkpoint` the partial dataset is saved every `every` graphs; with
+    `seconds` > 0 the sweep stops after that much wall time (what is done
+    is kept)."""
+    t_start = time.time()
     from concurrent.futures import ThreadPoolExecutor
     from . import Graph
     X, T, TT, info = [], [], [], []
@@ -333,8 +339,12 @@ def build_dataset(count: int, max_scale: int = 22, n_sources: int = 2, min_scale
             info.append(desc)
             log(f"[{i}] {desc} sweep {time.time() - t0:.1f}s")
             g.close()
-            if checkpoint and (len(X) % every == 0 or i + 1 == first + count):
+            out_of_time = seconds > 0 and time.time() - t_start > seconds
+            if checkpoint and (len(X) % every == 0 or i + 1 == first + count or out_of_time):
                 save_dataset(checkpoint, np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info)
+            if out_of_time:
+                log(f"stopped after {len(X)} graphs ({time.time() - t_start:.0f} s)")
+                break
     return np.array(X, np.float32), np.array(T, np.float32), np.array(TT), info
 
 
@@ -533,6 +543,7 @@ if __name__ == "__main__":
     ap.add_argument("--min-scale", type=int, default=14)
     ap.add_argument("--max-scale", type=int, default=22)
     ap.add_argument("--checkpoint", default=None, help="sweep only: save the partial dataset here")
+    ap.add_argument("--seconds", type=float, default=0.0, help="sweep only: stop after this much wall time")
     ap.add_argument("--merge", nargs="+", default=None, help="concatenate these sweep datasets into --dataset-out")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--dataset-out", default=None)
@@ -543,7 +554,8 @@ if __name__ == "__main__":
     elif a.from_dataset:
         train_from_dataset(a.from_dataset, out=a.out)
     elif a.checkpoint:
-        build_dataset(a.graphs, a.max_scale, min_scale=a.min_scale, first=a.first, checkpoint=a.checkpoint)
+        build_dataset(a.graphs, a.max_scale, min_scale=a.min_scale, first=a.first, checkpoint=a.checkpoint,
+                      seconds=a.seconds)
     else:
         X, T, TT, info = build_dataset(a.graphs, a.max_scale, min_scale=a.min_scale, first=a.first)
         if a.dataset_out:
