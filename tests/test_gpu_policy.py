@@ -150,3 +150,38 @@ def test_dead_zone_keeps_near_far_delta(pol, b2, cuda):
     assert p.decide(pol.graph_features(g))["delta_mult"] == pytest.approx(2.0 ** 0.375, rel=1e-6)
     pol.Policy.deactivate()
     g.close()
+
+
+def test_trained_policy_gains_on_held_out_graphs(pol, b2, orc, cuda):
+    """What the trained network gains over the method without it.  A policy is
+    trained with the library's own kernels on 80 % of the shipped sweep
+    dataset and decides for the held-out 20 %: the time of each decision, read
+    off that graph's measured sweep table, beats the fixed Near-Far schedule
+    in geometric mean.  Live solves with the decisions on regenerated
+    held-out graphs give the fixed schedule's distances word for word."""
+    import os
+    X, _, TT, info = pol.load_dataset(os.path.join(os.path.dirname(pol.DEFAULT_WEIGHTS), "policy_dataset.npz"))
+    idx = np.random.default_rng(11).permutation(len(X))
+    test, train = idx[: len(X) // 5], idx[len(X) // 5:]
+    T = np.array([pol.robust_label(a, 0.03) for a in TT], np.float32)
+    p = pol.Policy(seed=11)
+    p.train(X[train], T[train], epochs=800, lr=3e-3, weight_decay=1e-2)
+    Y = p.forward(X[test])
+    sp = np.array([pol.decision_speedup(TT[i], y) for i, y in zip(test, Y)])
+    gain = float(np.exp(np.log(sp).mean()))
+    best = float(np.exp(np.log([TT[i][pol.FIXED_INDEX] / TT[i].min() for i in test]).mean()))
+    assert gain > 1.0, (gain, best)
+    # live: the decisions change the schedule, never the distances
+    p.activate()
+    small = [i for i in test if info[i]["n"] <= (1 << 16)][:4]
+    for i in small:
+        hg, w, wtype, _ = pol.training_graph(int(info[i]["index"]))
+        g = b2.Graph.from_arrays(hg.rowptr, hg.colind, w, weight=wtype)
+        s = int(np.flatnonzero(np.diff(hg.rowptr))[0])
+        d0, _, _ = g.sssp(s)
+        d1, _, st = g.sssp(s, policy=1)
+        assert st["policy_used"] == 1
+        assert np.array_equal(d0.cpu().numpy().view(np.uint32), d1.cpu().numpy().view(np.uint32))
+        g.close()
+    pol.Policy.deactivate()
+    p.close()
