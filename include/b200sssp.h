@@ -145,7 +145,8 @@ typedef struct b2_sssp_opts {
                                exit) when the bucket's members hold more than pull_fraction x n
                                heavy out-edges (default 8); the incoming CSR is built on first
                                use, only for graphs with m >= pull_fraction x n; <= 0: push only */
-  uint32_t grid_blocks;     /* 0: occupancy-derived persistent grid */
+  uint32_t grid_blocks;     /* 0: the co-resident persistent grid (BF / delta: at most one thread
+                               per vertex on small graphs); k: at most k blocks */
   double timeout_ms;        /* bound on the whole solve and on every device wait, in ms
                                (default 20000; fractions of a millisecond allowed): past it the
                                kernel stops at its next wait or phase boundary and the call

@@ -1637,10 +1637,14 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
+  // small graphs: about one thread per vertex (every grid barrier costs an
+  // arrival per block, and a graph of a few thousand vertices cannot use more)
+  const int small_grid = (int)std::max<int64_t>(1, (g->n + kThreads - 1) / kThreads);
 #define B2_LAUNCH(WT, PR, MD)                                              \
   do {                                                                     \
     grid = max_grid<WT, PR, MD>();                                         \
     if (o.grid_blocks && (int)o.grid_blocks < grid) grid = o.grid_blocks;  \
+    else if (!o.grid_blocks && small_grid < grid) grid = small_grid;       \
     e = grid > 0 ? launch<WT, PR, MD>(P, grid, st) : cudaErrorInvalidConfiguration; \
   } while (0)
   if (mode == kModeBF) {
