@@ -200,7 +200,7 @@ __device__ __forceinline__ uint32_t sort_and_emit(const unsigned long long* __re
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRowWarps * 32)
+__global__ void __launch_bounds__(kRowWarps * 32, 4)
     k_rows_warp(int64_t M, int64_t N, const int64_t* __restrict__ arp, const int32_t* __restrict__ aci,
                 const T* __restrict__ av, const int64_t* __restrict__ brp, const int32_t* __restrict__ bci,
                 const T* __restrict__ bv, const unsigned long long* __restrict__ off, int32_t* __restrict__ tcol,
