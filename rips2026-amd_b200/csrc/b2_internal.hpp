@@ -135,13 +135,9 @@ struct Control {
   uint32_t local_iters;    // LOCAL phase: sub-phases run inside it
   uint32_t fusion_off;     // a LOCAL sub-phase scanned too many edges: no more fusion this solve
   uint32_t local_total;    // sub-phases run by all LOCAL phases
-  uint32_t far_min_key;    // adaptive mode: min distance key that landed in the far pile
-  uint32_t far_min_key_next;
-  unsigned long long win_frontier_sum;   // adaptive mode: frontier entries in this window
   unsigned long long member_heavy;       // heavy out-edges of the current bucket's members (push cost)
   uint32_t cur_min_key;                  // smallest label processed in the current bucket (pull bound)
   uint32_t heavy_pulls;                  // heavy passes run by pull
-  uint32_t win_phases;
   uint32_t delta_updates;
   // results
   uint32_t iterations;

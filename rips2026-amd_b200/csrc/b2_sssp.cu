@@ -107,8 +107,6 @@ struct Params {
   float pull_factor;      // pull when the members' heavy out-edges exceed pull_factor x n
   uint32_t is_float;
   uint32_t fusion;        // light frontiers up to this size run as a LOCAL phase (0: off)
-  uint32_t adapt;         // ADDS: adjust the bucket width at window boundaries
-  uint32_t adapt_cap;     // ADDS: frontier entries the grid takes per phase (utilization base)
   uint32_t dense_min;     // delta: near / slot frontiers of at least this many entries are swept
   uint32_t qcap;          // entries each worklist queue may hold (<= n; a push past it is kErrQueueOverflow)
   ProgressBoard* board;   // mapped progress record (null: no progress callback)
@@ -333,10 +331,6 @@ __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool i
     }
     bmin = __reduce_min_sync(0xffffffffu, bmin);
     if (lane_id() == 0 && bmin != 0xFFFFFFFFu) atomicMin(&c->far_min, bmin);
-    if (P.adapt) {
-      const uint32_t kmin = __reduce_min_sync(0xffffffffu, cls == 3 ? cand : 0xFFFFFFFFu);
-      if (lane_id() == 0 && kmin != 0xFFFFFFFFu) atomicMin(&c->far_min_key, kmin);
-    }
     stage(t.q.farb, t.q.nf, want, v);
     t.pushes += want ? 1 : 0;
   }
@@ -783,8 +777,6 @@ __device__ void manager_init(const Params& P) {
   r.dinv = __float_as_uint(P.inv_delta);
   r.dbase = 0;
   r.dbase_b = 0;
-  c->far_min_key = 0xFFFFFFFFu;
-  c->far_min_key_next = 0xFFFFFFFFu;
   c->cur_min_key = 0xFFFFFFFFu;
   c->member_heavy = 0;
   store_rec(c, r);
@@ -900,20 +892,56 @@ __device__ __forceinline__ void set_dense(const Params& P, PhaseRec& nx, uint32_
   }
 }
 
+// Every counter a delta manager step may read, loaded at once: independent
+// volatile loads issue back to back, so the step costs about one L2 round
+// trip instead of one per decision.
+struct MgrSnap {
+  uint32_t phases, probe_valid, local_q, local_total, local_iters, fusion_off, members, bucket_valid;
+  uint32_t iterations, heavy_pulls, far_min, far_min_next;
+  uint32_t hub[2], near[2], far[2], slot[kRing];
+  unsigned long long member_heavy;
+};
+__device__ __forceinline__ MgrSnap snapshot(const Control* c) {
+  MgrSnap m;
+  m.phases = vld(&c->phases);
+  m.probe_valid = vld(&c->probe_valid);
+  m.local_q = vld(&c->local_q);
+  m.local_total = vld(&c->local_total);
+  m.local_iters = vld(&c->local_iters);
+  m.fusion_off = vld(&c->fusion_off);
+  m.members = vld(&c->members_count);
+  m.bucket_valid = vld(&c->bucket_valid);
+  m.iterations = vld(&c->iterations);
+  m.heavy_pulls = vld(&c->heavy_pulls);
+  m.far_min = vld(&c->far_min);
+  m.far_min_next = vld(&c->far_min_next);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    m.hub[i] = vld(&c->hub_count[i]);
+    m.near[i] = vld(&c->near_count[i]);
+    m.far[i] = vld(&c->far_count[i]);
+  }
+#pragma unroll
+  for (int s = 0; s < kRing; ++s) m.slot[s] = vld(&c->slot_count[s]);
+  m.member_heavy = vld64(&c->member_heavy);
+  return m;
+}
+
 __device__ void manager_delta(const Params& P) {
   Control* c = P.ctl;
   const PhaseRec r = load_rec(c);
+  MgrSnap m = snapshot(c);
   trace_phase(P, r, r.cur);
   PhaseRec nx = r;
   nx.dense = kDenseOff;
   nx.fstamp = 0u;
   nx.phase = r.phase + 1;
   nx.stamp = P.phase_base + (c->stamp_ctr++);
-  c->phases = vld(&c->phases) + 1;
+  c->phases = m.phases + 1;
   if (r.kind == kPhaseFinal) { nx.kind = kPhaseDone; store_rec(c, nx); return; }
   if (over_budget(P, nx)) return;
   if (r.kind == kPhaseProbe) {
-    c->converged = vld(&c->probe_valid) ? 0u : 1u;
+    c->converged = m.probe_valid ? 0u : 1u;
     nx.kind = kPhaseFinal;
     store_rec(c, nx);
     return;
@@ -921,17 +949,13 @@ __device__ void manager_delta(const Params& P) {
   uint32_t win = r.win;
   uint32_t far_sel = r.far_sel;
   uint32_t from_slot = 0;   // first window slot to look at
-  if ((r.kind == kPhaseProcess || r.kind == kPhaseLocal) && !r.heavy) {
-    c->win_frontier_sum = c->win_frontier_sum + r.fcount;
-    c->win_phases = vld(&c->win_phases) + 1;
-  }
   if (r.kind == kPhaseSplit) {
     c->far_count[r.far_sel] = 0;
+    m.far[r.far_sel] = 0;
     far_sel = r.far_sel ^ 1u;
-    c->far_min = vld(&c->far_min_next);
+    c->far_min = m.far_min_next;
+    m.far_min = m.far_min_next;
     c->far_min_next = 0xFFFFFFFFu;
-    c->far_min_key = vld(&c->far_min_key_next);
-    c->far_min_key_next = 0xFFFFFFFFu;
     from_slot = 0;
   } else {  // PROCESS (light or heavy) or LOCAL
     PhaseRec rr = r;
@@ -939,17 +963,21 @@ __device__ void manager_delta(const Params& P) {
       // the local loop consumed every frontier it ran; its last pushes sit in local_q
       rr.fq = kQNone;
       rr.hub_in_chunks = 0;
-      rr.push_q = vld(&c->local_q);
+      rr.push_q = m.local_q;
       rr.heavy = 0;
-      c->local_total = vld(&c->local_total) + vld(&c->local_iters);
+      c->local_total = m.local_total + m.local_iters;
     }
     const PhaseRec& r = rr;
     consume_process_counters(c, r);
-    const uint32_t hch = vld(&c->hub_count[r.hub_out & 1]);
-    const uint32_t hcnt = hch;
-    const uint32_t nn = vld(&c->near_count[r.push_q & 1]);
+    // the same consumption in the snapshot
+    if (r.fq == kQNear0 || r.fq == kQNear1) m.near[r.fq] = 0;
+    else if (r.fq == kQMembers) m.members = 0;
+    else if (r.fq >= kQSlot0 && r.fq < kQSlot0 + kRing) m.slot[r.fq - kQSlot0] = 0;
+    if (r.hub_in_chunks) m.hub[r.hub_in & 1] = 0u;
+    const uint32_t hch = m.hub[r.hub_out & 1];
+    const uint32_t nn = m.near[r.push_q & 1];
     nx.hub_in = r.hub_out;
-    nx.hub_in_count = hcnt;
+    nx.hub_in_count = hch;
     nx.hub_in_chunks = hch;
     nx.hub_out = r.hub_out ^ 1u;
     if (r.heavy) {
@@ -977,21 +1005,20 @@ __device__ void manager_delta(const Params& P) {
         nx.fq = nn ? r.push_q : kQNone;
         nx.fcount = nn;
         nx.push_q = r.push_q ^ 1u;
-        if (hch == 0 && nn <= P.fusion && !vld(&c->fusion_off)) nx.kind = kPhaseLocal;
+        if (hch == 0 && nn <= P.fusion && !m.fusion_off) nx.kind = kPhaseLocal;
         // (a LOCAL phase's last pushes carry a stamp drawn inside it: no sweep after one)
         if (nn > 0 && r.kind != kPhaseLocal) set_dense(P, nx, kDenseNear, r.stamp);
         store_rec(c, nx);
         return;
       }
-      const uint32_t mc = vld(&c->members_count);
+      const uint32_t mc = m.members;
       if (mc > 0) {              // light rounds of this bucket are done: heavy pass
         nx.heavy = 1;
-        const unsigned long long mh = vld64(&c->member_heavy);
         c->member_heavy = 0;     // a later heavy pass of this bucket counts only its own members
-        if (P.in_rowptr && (double)mh > (double)P.pull_factor * (double)P.n) {
+        if (P.in_rowptr && (double)m.member_heavy > (double)P.pull_factor * (double)P.n) {
           // push would relax more heavy edges than a pull over every vertex costs
           c->members_count = 0;
-          c->heavy_pulls = vld(&c->heavy_pulls) + 1;
+          c->heavy_pulls = m.heavy_pulls + 1;
           nx.kind = kPhasePull;
           nx.fq = kQNone;
           nx.fcount = P.n;
@@ -1009,14 +1036,15 @@ __device__ void manager_delta(const Params& P) {
     // bucket r.cur is settled
     c->cur_min_key = 0xFFFFFFFFu;
     c->member_heavy = 0;
-    if (vld(&c->bucket_valid)) {
-      c->iterations = vld(&c->iterations) + 1;
+    if (m.bucket_valid) {
+      m.iterations += 1;
+      c->iterations = m.iterations;
       c->bucket_valid = 0;
       // the previous bucket had a successor (the reference's `changed`,
       // delta_stepping_hip_CSR.cpp:744-756); the last one is reported at the end
-      if (c->iterations > 1) publish_progress(P.board, c->iterations - 1, 1u, globaltimer_ns() - c->t_start);
+      if (m.iterations > 1) publish_progress(P.board, m.iterations - 1, 1u, globaltimer_ns() - c->t_start);
     }
-    if (vld(&c->iterations) >= P.max_iters) {
+    if (m.iterations >= P.max_iters) {
       nx.kind = kPhaseProbe;
       nx.heavy = 0;
       nx.hub_in_chunks = 0;
@@ -1026,12 +1054,9 @@ __device__ void manager_delta(const Params& P) {
     from_slot = r.cur - r.win + 1;
   }
   // next non-empty window slot
-  uint32_t cnts[kRing];
-#pragma unroll
-  for (int s = 0; s < kRing; ++s) cnts[s] = vld(&c->slot_count[s]);
   int found = -1;
   for (int s = (int)from_slot; s < kRing; ++s) {
-    if (cnts[s]) { found = s; break; }
+    if (m.slot[s]) { found = s; break; }
   }
   nx.heavy = 0;
   nx.hround = P.phase_base + nx.phase;
@@ -1045,50 +1070,26 @@ __device__ void manager_delta(const Params& P) {
     nx.win = win;
     nx.cur = win + (uint32_t)found;
     nx.fq = kQSlot0 + (uint32_t)found;
-    nx.fcount = cnts[found];
+    nx.fcount = m.slot[found];
     nx.push_q = kQNear0;   // both near queues are empty at a bucket boundary
-    if (nx.fcount <= P.fusion && !vld(&c->fusion_off)) nx.kind = kPhaseLocal;
+    if (nx.fcount <= P.fusion && !m.fusion_off) nx.kind = kPhaseLocal;
     set_dense(P, nx, kDenseSlot, nx.cur);
     store_rec(c, nx);
     return;
   }
-  const uint32_t fc = vld(&c->far_count[far_sel]);
+  const uint32_t fc = m.far[far_sel];
   if (fc > 0) {
-    const uint32_t fmin_b = vld(&c->far_min);
+    // the next aligned window holding the smallest far bucket
+    const uint32_t fmin_b = m.far_min;
     uint32_t nwin = win + kRing;
-    if (P.adapt) {
-      // ADDS feedback (hip_adds_sssp.hpp:41-56): widen buckets when the last
-      // window's frontiers left the grid under-used, narrow them when they
-      // overflowed it; the new window starts at the smallest far distance.
-      const unsigned long long ph = vld(&c->win_phases);
-      const double avg = ph ? (double)c->win_frontier_sum / (double)ph : 0.0;
-      double f = 1.0;
-      if (avg < 0.35 * (double)P.adapt_cap) f = 1.5;
-      else if (avg > 0.85 * (double)P.adapt_cap) f = 0.75;
-      if (f != 1.0) c->delta_updates = vld(&c->delta_updates) + 1;
-      if (P.is_float) {
-        const float wnew = fmaxf(1.0e-6f, (float)((1.0 / (double)__uint_as_float(r.dinv)) * f));
-        nx.dinv = __float_as_uint(1.0f / wnew);
-      } else {
-        const double wnew = fmax(1.0, floor((double)r.dq * f + 0.5));
-        nx.dq = (uint32_t)fmin(wnew, 4294967295.0);
-      }
-      const uint32_t kmin = vld(&c->far_min_key);
-      nx.dbase = kmin == 0xFFFFFFFFu ? r.dbase : (P.is_float ? __float_as_uint(key_to_f32(kmin)) : kmin);
-      nx.dbase_b = nwin;
-      c->win_frontier_sum = 0;
-      c->win_phases = 0;
-    } else {
-      const uint32_t aligned = (fmin_b / kRing) * kRing;
-      if (fmin_b != 0xFFFFFFFFu && aligned > nwin) nwin = aligned;
-    }
+    const uint32_t aligned = (fmin_b / kRing) * kRing;
+    if (fmin_b != 0xFFFFFFFFu && aligned > nwin) nwin = aligned;
     nx.kind = kPhaseSplit;
     nx.fq = kQFar0 + far_sel;
     nx.fcount = fc;
     nx.win = nwin;
     nx.cur = nwin;
     c->far_min_next = 0xFFFFFFFFu;
-    c->far_min_key_next = 0xFFFFFFFFu;
     store_rec(c, nx);
     return;
   }
@@ -1225,10 +1226,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
           if (b < R.win) { cls = 0; P.farflag[v] = 0u; }
           else if (b < R.win + (uint32_t)kRing) { cls = 2; P.farflag[v] = 0u; P.bstamp[v] = b; }
           else { cls = 3; kmin = min(kmin, b); P.bstamp[v] = b; }
-        }
-        if (P.adapt) {
-          const uint32_t km = __reduce_min_sync(0xffffffffu, cls == 3 ? k : 0xFFFFFFFFu);
-          if (lane_id() == 0 && km != 0xFFFFFFFFu) atomicMin(&c->far_min_key_next, km);
         }
         if (cls == 2) {
           const uint32_t s = b - R.win;
@@ -1477,7 +1474,7 @@ void progress_finish(b2_graph g, const b2_sssp_opts& o, int32_t max_iters, uint3
 }
 
 b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t* d_pred,
-                   const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats, bool adds = false) {
+                   const b2_sssp_opts* o_in, cudaStream_t st, b2_stats* stats) {
   if (!g || !d_dist) return B2_INVALID_ARGUMENT;
   if ((int64_t)source >= g->n) return B2_INVALID_ARGUMENT;
   b2_sssp_opts o;
@@ -1574,14 +1571,6 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     const float dfrac = o.dense_fraction != 0.0f ? o.dense_fraction : (g->max_degree <= 64 ? 1.0f / 16.0f : -1.0f);
     P.dense_min = dfrac > 0.0f ? (uint32_t)std::min(4294967295.0, std::max(1.0, std::ceil((double)dfrac * g->n)))
                                : 0xFFFFFFFFu;
-    if (adds) {
-      int dev = 0, sms = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      P.adapt = 1;
-      P.adapt_cap = (uint32_t)sms * 2u * (uint32_t)kThreads;
-      if (!policy_used && P.fusion == 0 && g->max_degree <= 64) P.fusion = 1024;   // low-degree graphs: fuse tails
-    }
     if (o.light_heavy && g->rows_sorted) {
       s = ensure_light_counts(g, isf, P.delta_u, df, st);
       if (s != B2_SUCCESS) return s;
