@@ -184,9 +184,9 @@ struct alignas(128) AddsControl {
   AddsSlot slot[kAddsSlots];
   // window epoch: written by the one warp that prepares a split while every
   // other warp waits; `epoch` is written last
-  uint32_t state;             // AddsState
+  uint32_t state_unused;
   uint32_t epoch;
-  uint32_t head;              // first bucket of the epoch not yet retired (0..kAddsSlots)
+  uint32_t head_unused;
   uint32_t W;                 // global number of slot 0's bucket
   uint32_t kbase;             // distance key at which slot 0 starts
   uint32_t dq;                // bucket width (uint32 graphs)
@@ -198,7 +198,12 @@ struct alignas(128) AddsControl {
   uint32_t pad1[20];
   unsigned long long hub_claim;   // hub chunks claimed
   unsigned long long hub_reserved;
-  uint32_t pad2[28];
+  // (epoch << 32) | position: the first bucket of the epoch not yet retired
+  // (0 .. kAddsSlots), or an AddsHead mark.  Every change of the window --
+  // retiring a bucket, ending the epoch, finishing the solve -- is a
+  // compare-and-swap of this one word, so a warp acting on a stale epoch fails.
+  unsigned long long head;
+  uint32_t pad2[26];
   uint32_t split_cursor;
   uint32_t split_done;
   uint32_t split_total;
@@ -219,7 +224,12 @@ struct alignas(128) AddsControl {
   uint32_t converged;
 };
 
-enum AddsState : uint32_t { kAddsRun = 0, kAddsSplitPrep = 1, kAddsSplit = 2, kAddsDone = 3 };
+// Marks in the position half of AddsControl::head.
+enum AddsHead : uint32_t {
+  kAddsPrep = 0xFFFFFFF0u,    // one warp prepares the next epoch; everyone else waits
+  kAddsSplit = 0xFFFFFFF1u,   // every warp routes far-pile entries into the new window
+  kAddsDone = 0xFFFFFFF2u,    // no work is left: labels are final
+};
 
 // Per-graph solver workspace, sized for n vertices (allocated on first use).
 struct Workspace {
