@@ -408,13 +408,13 @@ __device__ __forceinline__ void hub_chunk(const Params& P, const PhaseRec& R, ui
   const HubEntry* H = P.hubs + (size_t)(R.hub_in & 1) * P.hub_cap;
   const uint2 h = ldcg(reinterpret_cast<const uint2*>(H + item));
   const uint32_t v = h.x;
+  uint64_t rlo, rhi;
+  bool hh;
+  phase_range(P, R, v, rlo, rhi, hh);   // issued with the label load
   const uint32_t du = src_key<W, PRED, MODE>(P, v);
   bool valid = du != kInfKey;
   if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
   if (!valid) return;
-  uint64_t rlo, rhi;
-  bool hh;
-  phase_range(P, R, v, rlo, rhi, hh);
   const uint64_t e0 = rlo + (uint64_t)h.y * kHubChunk;
   const uint64_t e1 = min(rhi, e0 + kHubChunk);
   // B2_HUB_UNROLL edge loads per lane in flight per step
@@ -446,10 +446,16 @@ __device__ __forceinline__ void expand_vertices(const Params& P, const PhaseRec&
   uint64_t lo = 0, hi = 0, row_end = 0;
   bool valid = false, has_heavy = false;
   if (present) {
+    // the row bounds do not depend on the label: both loads go out together
+    // (one dependent memory round trip less per item)
+    phase_range(P, R, v, lo, hi, has_heavy, &row_end);
     du = src_key<W, PRED, MODE>(P, v);
     valid = du != kInfKey;
     if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
-    if (valid) phase_range(P, R, v, lo, hi, has_heavy, &row_end);
+    if (!valid) {
+      lo = hi = row_end = 0;
+      has_heavy = false;
+    }
   }
   if (MODE == kModeDelta) {
     if (__any_sync(0xffffffffu, valid) && lane == 0 && ldcg(&c->bucket_valid) == 0) c->bucket_valid = 1;
