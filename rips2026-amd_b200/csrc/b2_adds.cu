@@ -299,16 +299,14 @@ __device__ void expand(const AParams& P, const View& E, uint32_t v, bool take, u
   uint32_t du = kInfKey;
   uint64_t lo = 0, hi = 0;
   if (take) {
+    lo = __ldg(P.rowptr + v);   // row bounds go out with the label load
+    hi = __ldg(P.rowptr + v + 1);
     __threadfence();   // the qb reset is visible before the label is read
     du = L::key(ld_keep((const typename L::T*)P.dist + v, t.keep));
     // a label that has dropped into a lower bucket since this entry was
     // queued is expanded from there (it was queued there, or was expanded
     // there already with this label)
     if (du != kInfKey && slot_of<W>(E, du) < s) du = kInfKey;
-    if (du != kInfKey) {
-      lo = __ldg(P.rowptr + v);
-      hi = __ldg(P.rowptr + v + 1);
-    }
   }
   uint32_t deg = (du != kInfKey) ? (uint32_t)min(hi - lo, (uint64_t)0xFFFFFFFFull) : 0u;
   uint32_t hubs = __ballot_sync(kFull, deg >= P.hub_degree);
