@@ -51,6 +51,7 @@ constexpr int32_t kMiss32 = 1073741823;
 constexpr int32_t kDropCol = 0x7fffffff;   // sorts after every real column
 constexpr int kWarpRowMax = 512;           // candidates of a row sorted in one warp's registers
 constexpr int kRowWarps = 8;               // warps per block of k_rows_warp
+constexpr int kPairMax = 64;                // candidates of a row sorted by half a warp (k_rows_pair)
 constexpr unsigned long long kNoKey = ~0ull;
 
 enum SpStatus : uint32_t { kSpOk = 0, kSpBadIndex = 1, kSpBadRowptr = 2 };
@@ -213,10 +214,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4)
   for (int64_t i = warp; i < M; i += nwarps) {
     const unsigned long long o0 = off[i], ub = off[i + 1] - o0;
     if (ub > (unsigned long long)kWarpRowMax) continue;   // long row: expand-sort-compress
-    if (ub == 0) {
-      if (lane == 0) cnt[i] = 0;
-      continue;
-    }
+    if (ub <= (unsigned long long)kPairMax) continue;      // small row: k_rows_pair
     // gather: up to 32 A entries at a time; lane t holds entry t's B range
     uint32_t n = 0;
     const int64_t a0 = arp[i], a1 = arp[i + 1];
@@ -275,6 +273,153 @@ __global__ void __launch_bounds__(kRowWarps * 32, 4)
 }
 
 // ---- long rows: expand-sort-compress over a row list -----------------------
+// ---- small rows: two rows per warp, one per half-warp ----------------------
+// Rows with at most kPairMax candidates (every row of a sparse random graph)
+// take half a warp each, so a warp keeps two rows' dependent gathers in
+// flight.  Same steps as k_rows_warp inside 16 lanes: gather the row's
+// candidates as keys into shared memory, bitonic-sort 16 x 4 keys in
+// registers (shuffles never cross the half), emit the head of every column
+// run.  Loop trip counts are the larger half's, so every shuffle runs on the
+// full warp.
+
+template <typename T>
+__global__ void __launch_bounds__(kRowWarps * 32)
+    k_rows_pair(int64_t M, int64_t N, const int64_t* __restrict__ arp, const int32_t* __restrict__ aci,
+                const T* __restrict__ av, const int64_t* __restrict__ brp, const int32_t* __restrict__ bci,
+                const T* __restrict__ bv, const unsigned long long* __restrict__ off, int32_t* __restrict__ tcol,
+                T* __restrict__ tval, int64_t* __restrict__ cnt, uint32_t* status) {
+  __shared__ unsigned long long s_keys[kRowWarps][2][kPairMax];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t half = lane >> 4, hl = lane & 15u;
+  unsigned long long* sk = s_keys[threadIdx.x >> 5][half];
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i0 = warp * 2; i0 < M; i0 += nwarps * 2) {
+    const int64_t i = i0 + half;
+    unsigned long long o0 = 0, ub = 0;
+    if (i < M) {
+      o0 = off[i];
+      ub = off[i + 1] - o0;
+    }
+    const bool mine = i < M && ub <= (unsigned long long)kPairMax;   // other rows: k_rows_warp
+    int64_t a0 = 0, a1 = 0;
+    if (mine && ub > 0) {
+      a0 = arp[i];
+      a1 = arp[i + 1];
+    }
+    // gather, 16 A entries per pass
+    const int64_t alen = a1 - a0;
+    const int64_t alen_max = max(alen, (int64_t)__shfl_xor_sync(0xffffffffu, (long long)alen, 16));
+    uint32_t n = 0;
+    for (int64_t pa = 0; pa < alen_max; pa += 16) {
+      const int64_t p = a0 + pa + hl;
+      T a = T(0);
+      int64_t b0 = 0;
+      uint32_t len = 0;
+      if (pa + hl < alen) {
+        const int32_t k = aci[p];
+        a = av[p];
+        if (SpVal<T>::present(a)) {
+          b0 = brp[k];
+          len = (uint32_t)(brp[k + 1] - b0);
+        }
+      }
+      uint32_t incl = len;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o, 16);
+        if (hl >= (uint32_t)o) incl += y;
+      }
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 15, 16);
+      const uint32_t excl = incl - len;
+      const uint32_t total_max = max(total, __shfl_xor_sync(0xffffffffu, total, 16));
+      for (uint32_t s0 = 0; s0 < total_max; s0 += 16) {
+        const uint32_t sl = s0 + hl;
+        uint32_t t = 0;   // owner: the last lane of the half whose range starts at or before slot sl
+#pragma unroll
+        for (uint32_t step = 8; step >= 1; step >>= 1) {
+          const uint32_t e = __shfl_sync(0xffffffffu, excl, t + step, 16);
+          if (e <= sl) t += step;
+        }
+        const uint32_t ex_t = __shfl_sync(0xffffffffu, excl, t, 16);
+        const long long b0_t = __shfl_sync(0xffffffffu, (long long)b0, t, 16);
+        const T a_t = __shfl_sync(0xffffffffu, a, t, 16);
+        if (sl < total) {
+          const int64_t q = b0_t + (int64_t)(sl - ex_t);
+          const int32_t j = bci[q];
+          T c = T(0);
+          bool ok = SpVal<T>::combine(a_t, bv[q], c);
+          if (j < 0 || (int64_t)j >= N) {
+            atomicCAS(status, kSpOk, (uint32_t)kSpBadIndex);
+            ok = false;
+          }
+          sk[n + sl] = ok ? (((unsigned long long)(uint32_t)j << 32) | VKey<T>::enc(c)) : kNoKey;
+        }
+      }
+      n += total;
+    }
+    __syncwarp();
+    // sort 64 keys per half: element e = r * 16 + hl
+    constexpr int P = kPairMax / 16;
+    unsigned long long key[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      const uint32_t e = (uint32_t)r * 16u + hl;
+      key[r] = (mine && e < n) ? sk[e] : kNoKey;
+    }
+#pragma unroll
+    for (int k = 2; k <= kPairMax; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        if (j >= 16) {
+#pragma unroll
+          for (int r = 0; r < P; ++r) {
+            const int rp = r ^ (j >> 4);
+            if (rp > r) {
+              const bool up = ((r * 16) & k) == 0;
+              const unsigned long long x = key[r], y = key[rp];
+              if ((x > y) == up) {
+                key[r] = y;
+                key[rp] = x;
+              }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < P; ++r) {
+            const uint32_t e = (uint32_t)r * 16u + hl;
+            const bool up = (e & (uint32_t)k) == 0;
+            const unsigned long long o = shfl_xor64(key[r], j);
+            const bool lower = (hl & (uint32_t)j) == 0;
+            const bool take_min = lower == up;
+            key[r] = take_min ? (o < key[r] ? o : key[r]) : (o > key[r] ? o : key[r]);
+          }
+        }
+      }
+    }
+    // heads of column runs, in order
+    uint32_t kept = 0;
+    uint32_t carry = 0xFFFFFFFFu;
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      const uint32_t col = (uint32_t)(key[r] >> 32);
+      uint32_t pc = __shfl_up_sync(0xffffffffu, col, 1, 16);
+      if (hl == 0) pc = carry;
+      const bool head = mine && key[r] != kNoKey && col != pc;
+      const uint32_t b = __ballot_sync(0xffffffffu, head) & (half ? 0xFFFF0000u : 0x0000FFFFu);
+      if (head) {
+        const uint32_t pos = kept + __popc(b & ((1u << lane) - 1u));
+        tcol[o0 + pos] = (int32_t)col;
+        tval[o0 + pos] = VKey<T>::dec((uint32_t)key[r]);
+      }
+      kept += __popc(b);
+      carry = __shfl_sync(0xffffffffu, col, 15, 16);
+    }
+    if (mine && hl == 0) cnt[i] = kept;
+    __syncwarp();
+  }
+}
+
 template <typename T>
 __global__ void k_expand(int64_t L, const int64_t* __restrict__ rows, int64_t N, const int64_t* __restrict__ arp,
                          const int32_t* __restrict__ aci, const T* __restrict__ av, const int64_t* __restrict__ brp,
@@ -520,9 +665,17 @@ b2_status compute(const b2_csr* A, const b2_csr* B, cudaStream_t st, SpPlan& pla
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int64_t want = (M + kRowWarps - 1) / kRowWarps;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 6));
-    k_rows_warp<T><<<blocks, kRowWarps * 32, 0, st>>>(M, N, arp, A->colind, (const T*)A->values, brp, B->colind,
-                                                    (const T*)B->values, off.p, tcol.p, tval.p, cnt.p, status.p);
+    const int pair_blocks =
+        (int)std::max<int64_t>(1, std::min<int64_t>((M + 2 * kRowWarps - 1) / (2 * kRowWarps), (int64_t)sms * 16));
+    k_rows_pair<T><<<pair_blocks, kRowWarps * 32, 0, st>>>(M, N, arp, A->colind, (const T*)A->values, brp,
+                                                         B->colind, (const T*)B->values, off.p, tcol.p, tval.p,
+                                                         cnt.p, status.p);
     e = cudaGetLastError();
+    if (e == cudaSuccess) {
+      k_rows_warp<T><<<blocks, kRowWarps * 32, 0, st>>>(M, N, arp, A->colind, (const T*)A->values, brp, B->colind,
+                                                      (const T*)B->values, off.p, tcol.p, tval.p, cnt.p, status.p);
+      e = cudaGetLastError();
+    }
   } else {
     e = cudaMemsetAsync(cnt.p, 0, (size_t)M * sizeof(int64_t), st);
   }
