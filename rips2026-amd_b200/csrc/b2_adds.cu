@@ -62,9 +62,11 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;       // empty queue word
 constexpr unsigned long long kEmpty64 = ~0ull; // empty hub ring entry
 constexpr uint32_t kNotQueued = 0xFFFFFFFFu;   // qb[v]: not waiting in any bucket
-constexpr uint32_t kClaim = 64;                // entries a warp claims at once (two per lane)
+constexpr uint32_t kGrab = 32;                 // entries a warp takes from its block's pool (one per lane)
+constexpr uint32_t kBlockClaimMin = 64;        // entries a block claims from a bucket at once: its share
+constexpr uint32_t kBlockClaimMax = 1024;      //   of the bucket's unclaimed entries, within these bounds
 constexpr uint32_t kChunkEdges = 256;          // edges per hub chunk
-constexpr uint32_t kHubClaim = 2;              // hub chunks a warp claims at once
+constexpr uint32_t kHubClaim = 32;             // hub chunks a block claims at once
 constexpr int kU = 4;                          // edge slots per lane per step
 
 struct AParams {
@@ -194,18 +196,43 @@ __device__ unsigned long long wait_hub(const AParams& P, const unsigned long lon
 }
 
 // Append the wanting lanes' vertices to window slots (grouped by slot, one
-// atomic per group) -- warp-collective.
+// atomic per group) -- warp-collective.  A slot queue is a ring of `cap`
+// words: position p lives at p % cap.  Entries still unclaimed never exceed
+// the vertices waiting in the bucket (qb[] allows one per vertex), so a ring
+// of n words plus the claims in flight holds them; a push that finds the ring
+// full records kErrQueueOverflow (B2_POOL_EXHAUSTED).  The word at p % cap
+// was claimed with position p - cap; its taker writes it back to empty right
+// after reading it, so the writer waits (bounded) for that.
 __device__ __forceinline__ void push_slots(const AParams& P, bool want, uint32_t s, uint32_t v) {
   if (!__any_sync(kFull, want)) return;
   const uint32_t grp = __match_any_sync(kFull, want ? s : 0xFFFFFFFFu);
   if (!want) return;
   const uint32_t leader = __ffs(grp) - 1;
-  uint32_t base = 0;
-  if (lane_id() == leader) base = atomicAdd(&P.ctl->slot[s].reserved, (uint32_t)__popc(grp));
+  uint32_t base = 0, claimed = 0;
+  if (lane_id() == leader) {
+    base = atomicAdd(&P.ctl->slot[s].reserved, (uint32_t)__popc(grp));
+    claimed = (uint32_t)ld_vol64(&P.ctl->slot[s].claim);
+  }
   base = __shfl_sync(grp, base, leader);
+  claimed = __shfl_sync(grp, claimed, leader);
   const uint32_t pos = base + __popc(grp & ((1u << lane_id()) - 1u));
-  if (pos < P.cap) __stcg(slot_queue(P, s) + pos, v);
-  else set_err(P, kErrQueueOverflow, 42);
+  if (pos - claimed >= P.cap) {
+    set_err(P, kErrQueueOverflow, 42);
+    return;
+  }
+  uint32_t* w = slot_queue(P, s) + (pos % P.cap);
+  if (ld_vol(w) != kEmpty) {   // the previous lap's taker has not written it back yet
+    const uint64_t t0 = globaltimer_ns();
+    while (ld_vol(w) != kEmpty) {
+      __nanosleep(64);
+      if (ld_vol(&P.ctl->error)) return;
+      if (globaltimer_ns() - t0 > P.budget_ns) {
+        set_err(P, kErrTimeout, 46);
+        return;
+      }
+    }
+  }
+  __stcg(w, v);
 }
 
 // Append to the epoch's far pile -- warp-collective.
@@ -372,7 +399,7 @@ __device__ void take_entries(const AParams& P, const View& E, uint32_t s, uint32
     uint32_t v = 0;
     bool take = false;
     if (present) {
-      uint32_t* wp = slot_queue(P, s) + c + j0 + lane_id();
+      uint32_t* wp = slot_queue(P, s) + ((c + j0 + lane_id()) % P.cap);
       v = wait_word(P, wp);
       if (v != kEmpty) {
         __stcg(wp, kEmpty);
@@ -425,32 +452,116 @@ __device__ void take_chunk(const AParams& P, const View& E, unsigned long long p
   finish_units(P, s, 1);
 }
 
-// Claim hub chunks.  Returns 1 when work was done, 2 on a lost race, 0 when
-// the ring holds no unclaimed chunk.
-template <class W, bool PRED>
-__device__ int try_hub(const AParams& P, ATally& t) {
+__device__ __forceinline__ unsigned long long head_word(uint32_t epoch, uint32_t pos) {
+  return ((unsigned long long)epoch << 32) | pos;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// ---- per-block work pools --------------------------------------------------
+// Claims from the shared queues go through one warp per block: it claims up
+// to kBlockClaimMax entries of a bucket (or kHubClaim hub chunks) with one
+// compare-and-swap and publishes the range in shared memory, where the
+// block's warps take kGrab entries (or one chunk) at a time with shared
+// atomics.  A ticket is (generation << 32) | next; the range of a generation
+// sits in the descriptor of its parity, tagged with the generation, so a
+// ticket from a range that has been replaced finds a stale tag and is
+// dropped.
+struct PoolDesc {
+  unsigned long long base;   // first claimed position (entries: slot position; hubs: ring position)
+  uint32_t count;
+  uint32_t slot;             // entries: bucket slot
+  uint32_t gen;
+  uint32_t pad;
+};
+struct BlockPool {
+  unsigned long long ticket;   // entries
+  unsigned long long hticket;  // hub chunks
+  PoolDesc ent[2];
+  PoolDesc hub[2];
+  uint32_t lock;
+  uint32_t pos;                // head position the refilling warp saw last
+};
+
+__device__ __forceinline__ void publish_range(unsigned long long* ticket, PoolDesc* d, unsigned long long base,
+                                              uint32_t count, uint32_t slot) {
+  const uint32_t g = (uint32_t)(*(volatile unsigned long long*)ticket >> 32) + 1;
+  PoolDesc& x = d[g & 1];
+  x.base = base;
+  x.count = count;
+  x.slot = slot;
+  *(volatile uint32_t*)&x.gen = g;
+  __threadfence_block();
+  atomicExch(ticket, (unsigned long long)g << 32);
+}
+
+// Lane 0: take up to `want` items of the block's current range.  Returns the
+// count (0: empty or stale) with the first item's position and the slot.
+__device__ __forceinline__ uint32_t grab(unsigned long long* ticket, const PoolDesc* d, uint32_t want,
+                                         unsigned long long* first, uint32_t* slot) {
+  const unsigned long long t = atomicAdd(ticket, (unsigned long long)want);
+  const uint32_t g = (uint32_t)(t >> 32), i = (uint32_t)t;
+  const PoolDesc& x = d[g & 1];
+  const uint32_t cnt = *(const volatile uint32_t*)&x.count;
+  if (*(const volatile uint32_t*)&x.gen != g || i >= cnt) return 0;
+  *first = x.base + i;
+  *slot = x.slot;
+  return min(want, cnt - i);
+}
+
+__device__ __forceinline__ bool slot_complete(const AddsControl* c, uint32_t s);
+__device__ void idle_step(const AParams& P);
+
+// Lane 0 of the warp holding the block's lock: claim hub chunks, else
+// entries of the active buckets (lowest first), else do the idle step.
+// Returns true when a range was published.
+__device__ bool refill(const AParams& P, BlockPool& sp) {
   AddsControl* c = P.ctl;
-  unsigned long long cl = 0, k = 0;
-  int rc = 0;
-  if (lane_id() == 0) {
-    cl = ld_vol64(&c->hub_claim);
+  const unsigned long long hw = ld_acquire_u64(&c->head);
+  const uint32_t pos = (uint32_t)hw;
+  *(volatile uint32_t*)&sp.pos = pos;
+  if (pos > (uint32_t)kAddsSlots) return false;   // a split or the end
+  // hub chunks
+  for (int tries = 0; tries < 4; ++tries) {
+    const unsigned long long cl = ld_vol64(&c->hub_claim);
     const unsigned long long R = ld_vol64(&c->hub_reserved);
-    if (cl < R) {
-      k = min((unsigned long long)kHubClaim, R - cl);
-      if (atomicCAS(&c->hub_claim, cl, cl + k) == cl) rc = 1;
-      else { k = 0; rc = 2; }
+    if (cl >= R) break;
+    const unsigned long long k = min((unsigned long long)kHubClaim, R - cl);
+    if (atomicCAS(&c->hub_claim, cl, cl + k) == cl) {
+      publish_range(&sp.hticket, sp.hub, cl, (uint32_t)k, 0);
+      return true;
     }
   }
-  rc = __shfl_sync(kFull, rc, 0);
-  if (rc != 1) return rc;
-  cl = shfl64(cl, 0);
-  k = shfl64(k, 0);
-  // a claimed chunk pins its epoch (its bucket cannot complete): read it now
-  View E;
-  if (lane_id() == 0) E = read_view(c);
-  E = bcast(E);
-  for (unsigned long long i = 0; i < k; ++i) take_chunk<W, PRED>(P, E, cl + i, t);
-  return 1;
+  // entries
+  const uint32_t epoch = ld_vol(&c->epoch);
+  if ((uint32_t)(hw >> 32) == epoch && pos < (uint32_t)kAddsSlots) {
+    const uint32_t a = ld_vol(&c->active);
+    for (uint32_t j = 0; j < a && pos + j < (uint32_t)kAddsSlots; ++j) {
+      const uint32_t ss = pos + j;
+      for (int tries = 0; tries < 4; ++tries) {
+        const unsigned long long w = ld_vol64(&c->slot[ss].claim);
+        if ((uint32_t)(w >> 32) != epoch) return false;
+        const uint32_t got = (uint32_t)w;
+        const uint32_t R = ld_vol(&c->slot[ss].reserved);
+        if (got == R || (int32_t)(R - got) < 0) break;
+        const uint32_t avail = R - got;
+        const uint32_t share = avail / max(1u, gridDim.x);
+        const uint32_t k = min(avail, max(kBlockClaimMin, min(share, kBlockClaimMax)));
+        if (atomicCAS(&c->slot[ss].claim, w, w + k) == w) {
+          publish_range(&sp.ticket, sp.ent, got, k, ss);
+          return true;
+        }
+      }
+    }
+  }
+  idle_step(P);
+  return false;
 }
 
 __device__ __forceinline__ bool slot_complete(const AddsControl* c, uint32_t s) {
@@ -465,17 +576,6 @@ __device__ __forceinline__ bool claimable(const AddsControl* c, uint32_t s, uint
   return (uint32_t)(w >> 32) == epoch && (uint32_t)w < ld_vol(&c->slot[s].reserved);
 }
 
-__device__ __forceinline__ unsigned long long head_word(uint32_t epoch, uint32_t pos) {
-  return ((unsigned long long)epoch << 32) | pos;
-}
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
 
 // Lane 0 of the warp that moved the head from (epoch, kAddsSlots) to
 // (epoch, kAddsPrep): the next epoch, prepared while every warp waits; the
@@ -650,13 +750,13 @@ __device__ void idle_step(const AParams& P) {
 }
 
 template <class W, bool PRED>
-__device__ void worker(const AParams& P, ATally& t) {
+__device__ void worker(const AParams& P, BlockPool& sp, ATally& t) {
   AddsControl* c = P.ctl;
   uint32_t idle = 0;
   for (;;) {
     uint32_t pos = 0, err = 0;
     if (lane_id() == 0) {
-      pos = (uint32_t)ld_acquire_u64(&c->head);
+      pos = *(volatile uint32_t*)&sp.pos;
       err = ld_vol(&c->error);
       if (!err && globaltimer_ns() - ld_vol64(&c->t_start) > P.budget_ns) {
         set_err(P, kErrTimeout, 45);
@@ -667,56 +767,49 @@ __device__ void worker(const AParams& P, ATally& t) {
     err = __shfl_sync(kFull, err, 0);
     if (err || pos == kAddsDone) return;
     if (pos == kAddsSplit) {
-      if (split_work<W, PRED>(P)) idle = 0;
-      else __nanosleep(64);
-      continue;
-    }
-    if (pos == kAddsPrep) {
-      __nanosleep(64);
-      continue;
-    }
-    const int hr = try_hub<W, PRED>(P, t);
-    if (hr == 1) { idle = 0; continue; }
-    if (hr == 2) continue;
-    // entries from the active buckets, lowest first
-    View E;
-    uint32_t s = 0, cl = 0, k = 0;
-    if (lane_id() == 0) {
-      E = read_view(c);
-      const unsigned long long hw = ld_acquire_u64(&c->head);
-      const uint32_t h = (uint32_t)(hw >> 32) == E.epoch ? (uint32_t)hw : (uint32_t)kAddsSlots;
-      const uint32_t a = ld_vol(&c->active);
-      for (uint32_t j = 0; j < a && h + j < (uint32_t)kAddsSlots && k == 0; ++j) {
-        const uint32_t ss = h + j;
-        const unsigned long long w = ld_vol64(&c->slot[ss].claim);
-        if ((uint32_t)(w >> 32) != E.epoch) break;
-        const uint32_t got = (uint32_t)w;
-        const uint32_t R = min(ld_vol(&c->slot[ss].reserved), P.cap);
-        if (got >= R) continue;
-        const uint32_t kk = min(kClaim, R - got);
-        if (atomicCAS(&c->slot[ss].claim, w, w + kk) == w) {
-          s = ss;
-          cl = got;
-          k = kk;
-        } else {
-          k = 0xFFFFFFFFu;   // lost a race: look again
+      // every warp helps route the far pile; the block's pools are empty
+      if (!split_work<W, PRED>(P)) {
+        if (lane_id() == 0 && atomicCAS(&sp.lock, 0u, 1u) == 0u) {
+          *(volatile uint32_t*)&sp.pos = (uint32_t)ld_acquire_u64(&c->head);
+          atomicExch(&sp.lock, 0u);
         }
+        __syncwarp();
+        __nanosleep(128);
       }
+      continue;
     }
-    k = __shfl_sync(kFull, k, 0);
-    if (k == 0xFFFFFFFFu) continue;
-    if (k) {
+    // a hub chunk, else kGrab entries, from the block's pools
+    unsigned long long first = 0;
+    uint32_t slot = 0, k = 0, kind = 0;
+    if (lane_id() == 0) {
+      k = grab(&sp.hticket, sp.hub, 1, &first, &slot);
+      if (k) kind = 1;
+      else if ((k = grab(&sp.ticket, sp.ent, kGrab, &first, &slot)) != 0) kind = 2;
+    }
+    kind = __shfl_sync(kFull, kind, 0);
+    if (kind) {
+      first = shfl64(first, 0);
+      k = __shfl_sync(kFull, k, 0);
+      slot = __shfl_sync(kFull, slot, 0);
+      // a claimed unit pins its epoch (its bucket cannot complete): read it now
+      View E;
+      if (lane_id() == 0) E = read_view(c);
       E = bcast(E);
-      s = __shfl_sync(kFull, s, 0);
-      cl = __shfl_sync(kFull, cl, 0);
-      take_entries<W, PRED>(P, E, s, cl, k, t);
+      if (kind == 1) take_chunk<W, PRED>(P, E, first, t);
+      else take_entries<W, PRED>(P, E, slot, (uint32_t)first, k, t);
       idle = 0;
       continue;
     }
-    if (lane_id() == 0) idle_step(P);
-    __syncwarp();
+    // both pools are empty: one warp of the block refills them
+    uint32_t got = 0;
+    if (lane_id() == 0 && atomicCAS(&sp.lock, 0u, 1u) == 0u) {
+      got = refill(P, sp) ? 1u : 0u;
+      atomicExch(&sp.lock, 0u);
+    }
+    got = __shfl_sync(kFull, got, 0);
+    if (got) { idle = 0; continue; }
     ++idle;
-    __nanosleep(idle < 8 ? 32u : (idle < 64 ? 128u : 512u));
+    __nanosleep(idle < 4 ? 64u : (idle < 32 ? 256u : 1024u));
   }
 }
 
@@ -781,8 +874,12 @@ __global__ void __launch_bounds__(kAThreads, 2) k_adds(AParams P) {
   }
   ATally t;
   t.keep = l2_keep_policy();
+  __shared__ BlockPool sp;
+  if (threadIdx.x == 0) {
+    memset(&sp, 0, sizeof(sp));   // empty pools (generation 0, no items), position 0
+  }
   const bool ok = grid_barrier((GridBarrier*)c, gridDim.x, P.budget_ns, [&] { init_start<PRED>(P); });
-  if (ok) worker<W, PRED>(P, t);
+  if (ok) worker<W, PRED>(P, sp, t);
   // tallies (one atomic per warp)
   unsigned long long e = t.edges, im = t.impr, pu = t.pushes, en = t.entries, ch = t.chunks;
 #pragma unroll
@@ -844,7 +941,10 @@ cudaError_t launch_adds(const AParams& P, int grid, cudaStream_t st) {
 b2_status ensure_adds(b2_graph g, uint32_t cap_opt, cudaStream_t st) {
   Workspace& w = g->ws;
   const size_t n = (size_t)g->n;
-  const size_t cap = (cap_opt > 0 && cap_opt < n) ? cap_opt : n;
+  // a bucket ring holds the entries of its waiting vertices (at most n) plus
+  // slack for claim counts read while other blocks claim
+  const size_t full = n + std::min<size_t>(n, (size_t)1 << 19) + 1024;
+  const size_t cap = (cap_opt > 0 && cap_opt < full) ? cap_opt : full;
   if (w.adds_q && w.adds_cap == cap) return B2_SUCCESS;
   free_adds_workspace(w);
   cudaError_t e = cudaMalloc((void**)&w.adds_q, std::max<size_t>((size_t)(kAddsSlots + 2) * cap * 4, 16));
@@ -967,7 +1067,7 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   else grid = pred ? adds_grid<WU32, true>() : adds_grid<WU32, false>();
   if (o.grid_blocks && (int)o.grid_blocks < grid) grid = (int)o.grid_blocks;
   if (grid <= 0) return B2_CUDA_ERROR;
-  P.adapt_cap = (uint32_t)grid * (kAThreads / 32) * kClaim;
+  P.adapt_cap = (uint32_t)grid * (kAThreads / 32) * kGrab;   // one grab per warp fills the grid
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->delta_used = delta;
