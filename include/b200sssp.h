@@ -219,7 +219,7 @@ typedef struct b2_stats {
   uint32_t heavy_pulls;     /* heavy passes run in the pull direction */
   uint64_t work_items;      /* ADDS: bucket-queue entries and hub chunks taken by warps */
   uint32_t active_buckets_max; /* ADDS: widest range of buckets warps took entries from */
-  uint32_t reserved0;
+  uint32_t device_error_site; /* where in the kernel device_error was raised (0: none) */
 } b2_stats;
 
 /* ---- library ---------------------------------------------------------- */

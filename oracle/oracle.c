@@ -288,15 +288,31 @@ void orc_minplus_gemm_i32(const int32_t* A, const int32_t* B, int32_t* Cm, int64
 /* ---- CSR x CSR min-plus -------------------------------------------------
  * Returns nnz(C); C arrays must hold `cap` entries (call with cap = 0 to size).
  * Dense accumulator per row (fine for the oracle's small sizes). */
+/* columns touched by one output row (sorted before the row is written) */
+typedef struct { int32_t* a; int64_t n, cap; } cols_t;
+static void cols_push(cols_t* t, int32_t j) {
+  if (t->n == t->cap) {
+    t->cap = t->cap ? t->cap * 2 : 256;
+    t->a = (int32_t*)realloc(t->a, (size_t)t->cap * sizeof(int32_t));
+  }
+  t->a[t->n++] = j;
+}
+static int cmp_i32(const void* x, const void* y) {
+  const int32_t a = *(const int32_t*)x, b = *(const int32_t*)y;
+  return (a > b) - (a < b);
+}
+
 int64_t orc_minplus_spgemm_f32(int64_t M, int64_t K, int64_t N, const int64_t* arp, const int32_t* aci,
                                const float* av, const int64_t* brp, const int32_t* bci, const float* bv,
                                int64_t* crp, int32_t* cci, float* cv, int64_t cap) {
   float* acc = (float*)malloc((size_t)(N > 0 ? N : 1) * sizeof(float));
   unsigned char* has = (unsigned char*)calloc((size_t)(N > 0 ? N : 1), 1);
+  cols_t t = {0, 0, 0};
   int64_t nnz = 0;
   (void)K;
   for (int64_t i = 0; i < M; ++i) {
     if (crp) crp[i] = nnz;
+    t.n = 0;
     for (int64_t p = arp[i]; p < arp[i + 1]; ++p) {
       const float a = av[p];
       if (a != a || a == INFINITY) continue;
@@ -305,20 +321,22 @@ int64_t orc_minplus_spgemm_f32(int64_t M, int64_t K, int64_t N, const int64_t* a
         volatile float c = a + bv[q];
         if (c != c || c == INFINITY) continue;
         const int32_t j = bci[q];
-        if (!has[j]) { has[j] = 1; acc[j] = c; }
+        if (!has[j]) { has[j] = 1; acc[j] = c; cols_push(&t, j); }
         else if (c < acc[j]) acc[j] = c;
       }
     }
-    for (int64_t j = 0; j < N; ++j)
-      if (has[j]) {
-        if (cci && nnz < cap) { cci[nnz] = (int32_t)j; cv[nnz] = acc[j]; }
-        ++nnz;
-        has[j] = 0;
-      }
+    qsort(t.a, (size_t)t.n, sizeof(int32_t), cmp_i32);
+    for (int64_t x = 0; x < t.n; ++x) {
+      const int32_t j = t.a[x];
+      if (cci && nnz < cap) { cci[nnz] = j; cv[nnz] = acc[j]; }
+      ++nnz;
+      has[j] = 0;
+    }
   }
   if (crp) crp[M] = nnz;
   free(acc);
   free(has);
+  free(t.a);
   return nnz;
 }
 
@@ -329,10 +347,12 @@ int64_t orc_minplus_spgemm_i32(int64_t M, int64_t K, int64_t N, const int64_t* a
   const int64_t miss = 1073741823;
   int64_t* acc = (int64_t*)malloc((size_t)(N > 0 ? N : 1) * sizeof(int64_t));
   unsigned char* has = (unsigned char*)calloc((size_t)(N > 0 ? N : 1), 1);
+  cols_t t = {0, 0, 0};
   int64_t nnz = 0;
   (void)K;
   for (int64_t i = 0; i < M; ++i) {
     if (crp) crp[i] = nnz;
+    t.n = 0;
     for (int64_t p = arp[i]; p < arp[i + 1]; ++p) {
       const int64_t a = av[p];
       if (a >= miss) continue;
@@ -343,20 +363,22 @@ int64_t orc_minplus_spgemm_i32(int64_t M, int64_t K, int64_t N, const int64_t* a
         const int64_t c = a + b;
         if (c >= miss) continue;
         const int32_t j = bci[q];
-        if (!has[j]) { has[j] = 1; acc[j] = c; }
+        if (!has[j]) { has[j] = 1; acc[j] = c; cols_push(&t, j); }
         else if (c < acc[j]) acc[j] = c;
       }
     }
-    for (int64_t j = 0; j < N; ++j)
-      if (has[j]) {
-        if (cci && nnz < cap) { cci[nnz] = (int32_t)j; cv[nnz] = (int32_t)acc[j]; }
-        ++nnz;
-        has[j] = 0;
-      }
+    qsort(t.a, (size_t)t.n, sizeof(int32_t), cmp_i32);
+    for (int64_t x = 0; x < t.n; ++x) {
+      const int32_t j = t.a[x];
+      if (cci && nnz < cap) { cci[nnz] = j; cv[nnz] = (int32_t)acc[j]; }
+      ++nnz;
+      has[j] = 0;
+    }
   }
   if (crp) crp[M] = nnz;
   free(acc);
   free(has);
+  free(t.a);
   return nnz;
 }
 

@@ -270,9 +270,11 @@ class Graph:
             o.progress = C.cast(keep, C.c_void_p)
         st = _lib.Stats()
         fn = getattr(lib(), _METHODS[method])
-        check(fn(self._h, source, C.c_void_p(dist.data_ptr()),
-                 C.c_void_p(pr.data_ptr() if pr is not None else 0), C.byref(o),
-                 C.c_void_p(_stream_ptr(stream)), C.byref(st)), f"sssp[{method}]")
+        rc = fn(self._h, source, C.c_void_p(dist.data_ptr()),
+                C.c_void_p(pr.data_ptr() if pr is not None else 0), C.byref(o),
+                C.c_void_p(_stream_ptr(stream)), C.byref(st))
+        site = f" at device site {st.device_error_site}" if rc != _lib.SUCCESS and st.device_error_site else ""
+        check(rc, f"sssp[{method}]{site}")
         del keep
         return dist, pr, st.as_dict()
 

@@ -79,7 +79,7 @@ class Stats(C.Structure):
                 ("grid_blocks", C.c_uint32), ("first_unchanged", C.c_uint32),
                 ("local_subphases", C.c_uint32), ("delta_updates", C.c_uint32),
                 ("delta_final", C.c_double), ("policy_used", C.c_uint32), ("heavy_pulls", C.c_uint32),
-                ("work_items", C.c_uint64), ("active_buckets_max", C.c_uint32), ("reserved0", C.c_uint32)]
+                ("work_items", C.c_uint64), ("active_buckets_max", C.c_uint32), ("device_error_site", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

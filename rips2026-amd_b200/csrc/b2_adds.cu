@@ -5,38 +5,44 @@
 // hip_adds_sssp.cpp:460-866) runs a manager thread block that hands ranges of
 // paged bucket queues to idle worker blocks, and the ADS float port
 // (Charlotte_ADS_Float_Attempt/kernel.hip:66-221, wl.h:1833-1915) pushes into
-// 32 priority bags with warp-aggregated appends.  Here every warp of the grid
-// is a worker and there is no manager: warps claim work straight from the
-// bucket queues with one compare-and-swap per 64 entries, so no warp waits
-// for a single thread to scan the others.
+// 32 priority bags with warp-aggregated appends.  Here there is no manager:
+// one warp per block claims a range of up to 1024 entries of a bucket (or 32
+// hub chunks) with one compare-and-swap and parks it in a shared-memory pool,
+// from which the block's warps take 32 entries (or one chunk) at a time.
 //
 // Worklist.  A window epoch maps kAddsSlots consecutive buckets of width delta
 // to slots 0..kAddsSlots-1 (global bucket W + s); keys past the window go to a
-// far pile.  Each slot is an append-only queue with three counters on its own
-// cache line: `reserved` (entries writers reserved), `extra` (hub chunks its
-// entries spawned) and `done` (entries and chunks finished), plus a `claim`
-// word (epoch << 32 | entries claimed).  A bucket is complete when done ==
-// reserved + extra: every unit of its work is finished, and since a
+// far pile.  Each slot is a ring of position-tagged words with three counters
+// on its own cache line: `reserved` (positions writers reserved), `extra` (hub
+// chunks its entries spawned) and `done` (entries and chunks finished), plus a
+// `claim` word (epoch << 32 | positions claimed).  A bucket is complete when
+// done == reserved + extra: every unit of its work is finished, and since a
 // relaxation never lowers a key below its source's bucket, nothing can push
-// into it again once every lower bucket is complete.  The head bucket retires
-// as soon as it is complete; warps take entries from the `active` buckets
-// starting at the head (the reference's dynamic active-bucket count,
-// hip_adds_sssp.cpp:609-647, grows here when warps idle while later buckets
-// hold work).  When the whole window has retired, the one warp that wins a
-// compare-and-swap prepares the next epoch (new bucket width from the
-// epoch's utilization, the reference's growth 1.5 / shrink 0.75 feedback,
-// hip_adds_sssp.hpp:41-56) and every warp helps move the far pile into it.
+// into it again once every lower bucket is complete.
 //
-// Entries.  Queue words start empty (all ones); a writer reserves positions
-// with one atomic per slot group of a warp (__match_any_sync) and stores the
-// vertex; the consumer waits for the word to turn non-empty (bounded), takes
-// it and writes it back to empty, so a finished solve leaves every queue
-// empty.  A per-vertex word qb[v] holds the lowest bucket v is queued in and
-// not yet taken: a push happens only when it lowers qb[v], and a warp that
-// takes v from bucket b expands it unless qb[v] is below b (v then waits in
-// a lower bucket with its newer label).  Fences order the label atomic before
-// the qb update on the push side and the qb reset before the label read on
-// the take side, so an improvement is never left unexpanded.
+// Window state.  One 64-bit head word (epoch << 32 | position) holds the
+// lowest bucket not yet retired, or PREP / SPLIT / DONE.  Warps take entries
+// from the `active` buckets starting at the head (the reference's dynamic
+// active-bucket count, hip_adds_sssp.cpp:609-647, grows here when warps idle
+// while later buckets hold work).  An idle warp retires the complete head
+// bucket; when the whole window has retired, the warp that wins the
+// compare-and-swap to PREP sets up the next epoch (new bucket width from the
+// epoch's utilization, the reference's growth 1.5 / shrink 0.75 feedback,
+// hip_adds_sssp.hpp:41-56), and every warp helps route the far pile into it.
+// Each change is a compare-and-swap of the head word, so a warp holding a
+// stale view changes nothing.
+//
+// Entries.  Ring words start empty (all ones).  A writer reserves positions
+// with one atomic per slot group of a warp (__match_any_sync), waits (bounded)
+// for the word of the previous lap to be taken, and stores position << 32 |
+// vertex; the taker of position p waits for the word tagged p, takes it and
+// writes it back to empty, so a finished solve leaves every ring empty.  A
+// per-vertex word qb[v] holds the lowest bucket v is queued in and not yet
+// taken: a push happens only when it lowers qb[v], and a warp that takes v
+// from bucket b expands it unless qb[v] is below b (v then waits in a lower
+// bucket with its newer label).  Fences order the label atomic before the qb
+// update on the push side and the qb reset before the label read on the take
+// side, so an improvement is never left unexpanded.
 //
 // High-degree vertices are split into chunks of kChunkEdges edges in a ring
 // that any warp may take (counted in their bucket's `extra` before they are
@@ -59,8 +65,8 @@ namespace {
 
 constexpr int kAThreads = 512;
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr uint32_t kEmpty = 0xFFFFFFFFu;       // empty queue word
-constexpr unsigned long long kEmpty64 = ~0ull; // empty hub ring entry
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;       // no vertex: a wait gave up
+constexpr unsigned long long kEmpty64 = ~0ull; // empty ring word (bucket rings and the hub ring)
 constexpr uint32_t kNotQueued = 0xFFFFFFFFu;   // qb[v]: not waiting in any bucket
 constexpr uint32_t kGrab = 32;                 // entries a warp takes from its block's pool (one per lane)
 constexpr uint32_t kBlockClaimMin = 64;        // entries a block claims from a bucket at once: its share
@@ -77,7 +83,8 @@ struct AParams {
   void* dist;              // labels (keys, or key|pred words)
   uint32_t* qb;
   uint32_t* farflag;
-  uint32_t* q;             // kAddsSlots window queues, then the two far piles; cap entries each
+  unsigned long long* q;   // kAddsSlots window rings of cap tagged words (position << 32 | vertex)
+  uint32_t* far;           // the two far piles, cap entries each
   uint32_t cap;
   unsigned long long* hub; // ring of {v, chunk << 5 | slot}
   uint32_t hub_cap;
@@ -154,20 +161,25 @@ __device__ __forceinline__ uint32_t slot_of(const View& E, uint32_t key) {
   return b < 0.0f ? 0u : (uint32_t)b;
 }
 
-__device__ __forceinline__ uint32_t* slot_queue(const AParams& P, uint32_t s) { return P.q + (size_t)s * P.cap; }
-__device__ __forceinline__ uint32_t* far_queue(const AParams& P, uint32_t f) {
-  return P.q + (size_t)(kAddsSlots + f) * P.cap;
+__device__ __forceinline__ unsigned long long* slot_queue(const AParams& P, uint32_t s) {
+  return P.q + (size_t)s * P.cap;
+}
+__device__ __forceinline__ uint32_t* far_queue(const AParams& P, uint32_t f) { return P.far + (size_t)f * P.cap; }
+__device__ __forceinline__ unsigned long long ring_word(uint32_t pos, uint32_t v) {
+  return ((unsigned long long)pos << 32) | v;
 }
 
-// Bounded wait for a reserved queue word to be written.
-__device__ uint32_t wait_word(const AParams& P, const uint32_t* p) {
-  uint32_t v = ld_vol(p);
-  if (v != kEmpty) return v;
+// Bounded wait for the entry of ring position `pos` to be written at p; returns
+// its vertex (kEmpty: the wait gave up).  The tag keeps a consumer from taking
+// the previous lap's entry that still sits in the word.
+__device__ uint32_t wait_word(const AParams& P, const unsigned long long* p, uint32_t pos) {
+  unsigned long long w = ld_vol64(p);
+  if ((uint32_t)(w >> 32) == pos && w != kEmpty64) return (uint32_t)w;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 0;; ++i) {
     __nanosleep(32);
-    v = ld_vol(p);
-    if (v != kEmpty) return v;
+    w = ld_vol64(p);
+    if ((uint32_t)(w >> 32) == pos && w != kEmpty64) return (uint32_t)w;
     if ((i & 63u) == 63u) {
       if (ld_vol(&P.ctl->error)) return kEmpty;
       if (globaltimer_ns() - t0 > P.budget_ns) {
@@ -197,12 +209,14 @@ __device__ unsigned long long wait_hub(const AParams& P, const unsigned long lon
 
 // Append the wanting lanes' vertices to window slots (grouped by slot, one
 // atomic per group) -- warp-collective.  A slot queue is a ring of `cap`
-// words: position p lives at p % cap.  Entries still unclaimed never exceed
-// the vertices waiting in the bucket (qb[] allows one per vertex), so a ring
-// of n words plus the claims in flight holds them; a push that finds the ring
-// full records kErrQueueOverflow (B2_POOL_EXHAUSTED).  The word at p % cap
-// was claimed with position p - cap; its taker writes it back to empty right
-// after reading it, so the writer waits (bounded) for that.
+// 64-bit words: position p lives at p % cap, tagged with p.  Entries still
+// unclaimed never exceed the vertices waiting in the bucket (qb[] allows one
+// per vertex), so a ring of n words plus the claims in flight holds them; a
+// push that finds the ring full records kErrQueueOverflow (B2_POOL_EXHAUSTED).
+// The word at p % cap held position p - cap, claimed already; its taker writes
+// it back to empty right after reading it, so the writer waits (bounded) for
+// that.  Only the taker of p reads a word tagged p, so a slow taker of p - cap
+// never sees p's entry and no entry is taken twice or erased.
 __device__ __forceinline__ void push_slots(const AParams& P, bool want, uint32_t s, uint32_t v) {
   if (!__any_sync(kFull, want)) return;
   const uint32_t grp = __match_any_sync(kFull, want ? s : 0xFFFFFFFFu);
@@ -216,14 +230,16 @@ __device__ __forceinline__ void push_slots(const AParams& P, bool want, uint32_t
   base = __shfl_sync(grp, base, leader);
   claimed = __shfl_sync(grp, claimed, leader);
   const uint32_t pos = base + __popc(grp & ((1u << lane_id()) - 1u));
-  if (pos - claimed >= P.cap) {
+  // blocks may claim this warp's positions before the claim count is read:
+  // a negative distance is no overflow
+  if ((int32_t)(pos - claimed) >= (int32_t)P.cap) {
     set_err(P, kErrQueueOverflow, 42);
     return;
   }
-  uint32_t* w = slot_queue(P, s) + (pos % P.cap);
-  if (ld_vol(w) != kEmpty) {   // the previous lap's taker has not written it back yet
+  unsigned long long* w = slot_queue(P, s) + (pos % P.cap);
+  if (ld_vol64(w) != kEmpty64) {   // the previous lap's taker has not written it back yet
     const uint64_t t0 = globaltimer_ns();
-    while (ld_vol(w) != kEmpty) {
+    while (ld_vol64(w) != kEmpty64) {
       __nanosleep(64);
       if (ld_vol(&P.ctl->error)) return;
       if (globaltimer_ns() - t0 > P.budget_ns) {
@@ -232,7 +248,7 @@ __device__ __forceinline__ void push_slots(const AParams& P, bool want, uint32_t
       }
     }
   }
-  __stcg(w, v);
+  __stcg(w, ring_word(pos, v));
 }
 
 // Append to the epoch's far pile -- warp-collective.
@@ -247,26 +263,10 @@ __device__ __forceinline__ void push_far(const AParams& P, const View& E, bool w
   if (lane_id() == 0 && km != 0xFFFFFFFFu) atomicMin(&P.ctl->far_min_key, km);
 }
 
-// Queue one improvement per lane (warp-collective; `improved` may be false).
-template <class W>
-__device__ __forceinline__ void route(const AParams& P, const View& E, bool improved, uint32_t v, uint32_t cand,
-                                      ATally& t) {
-  if (!__any_sync(kFull, improved)) return;
-  uint32_t s = kAddsSlots;
-  bool want = false;
-  if (improved) {
-    s = slot_of<W>(E, cand);
-    const uint32_t gb = E.W + s;   // W + kAddsSlots marks "waiting in the far pile"
-    __threadfence();               // the label update is visible before the queue mark
-    want = atomicMin(&P.qb[v], gb) > gb;
-    if (want && s == kAddsSlots) want = atomicExch(&P.farflag[v], 1u) == 0u;
-  }
-  push_slots(P, want && s < kAddsSlots, s, v);
-  push_far(P, E, want && s == kAddsSlots, v, cand);
-  t.pushes += want ? 1 : 0;
-}
-
-// Relax kU edge slots per lane: loads first, then atomics, then queueing.
+// Relax kU edge slots per lane: label loads, then the label atomics of every
+// slot (issued before any result is read), one fence, then the queue marks
+// (again all issued first) and the pushes.  A push happens only when it
+// lowers qb[v]; the fence makes the label updates visible before their marks.
 template <class W, bool PRED>
 __device__ __forceinline__ void relax_route(const AParams& P, const View& E, const bool (&act)[kU],
                                             const uint32_t (&src)[kU], const uint32_t (&dsrc)[kU],
@@ -274,28 +274,56 @@ __device__ __forceinline__ void relax_route(const AParams& P, const View& E, con
   using L = Label<PRED>;
   typename L::T* lab = (typename L::T*)P.dist;
   uint32_t cand[kU];
-  typename L::T cur[kU];
+  typename L::T cur[kU], old[kU];
   bool imp[kU];
 #pragma unroll
   for (int q = 0; q < kU; ++q) {
     cand[q] = act[q] ? W::extend(dsrc[q], ed[q].y) : kInfKey;
-    cur[q] = (cand[q] != kInfKey) ? ld_keep(lab + ed[q].x, t.keep) : L::kInf;
+    cur[q] = ld_keep_if(cand[q] != kInfKey, lab + ed[q].x, t.keep, L::kInf);
   }
 #pragma unroll
   for (int q = 0; q < kU; ++q) {
-    imp[q] = false;
-    if (cand[q] != kInfKey) {
-      const typename L::T cw = L::make(cand[q], src[q]);
-      if (cw < cur[q]) {
-        const typename L::T old = atom_min_keep(lab + ed[q].x, cw, t.keep);
-        imp[q] = cand[q] < L::key(old);
-      }
-    }
+    const typename L::T cw = L::make(cand[q], src[q]);
+    // not issued: old = 0 reads as "no improvement"
+    old[q] = atom_min_keep_if(cand[q] != kInfKey && cw < cur[q], lab + ed[q].x, cw, t.keep, (typename L::T)0);
+  }
+  bool any_imp = false;
+#pragma unroll
+  for (int q = 0; q < kU; ++q) {
+    imp[q] = cand[q] < L::key(old[q]);
+    any_imp = any_imp || imp[q];
     t.edges += act[q] ? 1 : 0;
     t.impr += imp[q] ? 1 : 0;
   }
+  if (!__any_sync(kFull, any_imp)) return;
+  __threadfence();
+  uint32_t s[kU], oq[kU];
 #pragma unroll
-  for (int q = 0; q < kU; ++q) route<W>(P, E, imp[q], ed[q].x, cand[q], t);
+  for (int q = 0; q < kU; ++q) {
+    s[q] = imp[q] ? slot_of<W>(E, cand[q]) : (uint32_t)kAddsSlots;
+    // W + kAddsSlots marks "waiting in the far pile"; not issued: 0 reads as "queued lower"
+    oq[q] = atom_min_if(imp[q], &P.qb[ed[q].x], E.W + s[q], 0u);
+  }
+  uint32_t of[kU], kfar = 0xFFFFFFFFu;
+#pragma unroll
+  for (int q = 0; q < kU; ++q) {
+    const bool far = imp[q] && s[q] == kAddsSlots && oq[q] > E.W + s[q];
+    of[q] = atom_exch_if(far, &P.farflag[ed[q].x], 1u, 1u);
+    // every improvement past the window bounds the next epoch's base, also
+    // one whose vertex already waits in the far pile with an older key
+    if (imp[q] && s[q] == kAddsSlots) kfar = min(kfar, cand[q]);
+  }
+  kfar = __reduce_min_sync(kFull, kfar);
+  if (lane_id() == 0 && kfar != 0xFFFFFFFFu) atomicMin(&P.ctl->far_min_key, kfar);
+#pragma unroll
+  for (int q = 0; q < kU; ++q) {
+    const bool lowered = imp[q] && oq[q] > E.W + s[q];
+    const bool to_slot = lowered && s[q] < kAddsSlots;
+    const bool to_far = lowered && s[q] == kAddsSlots && of[q] == 0u;
+    push_slots(P, to_slot, s[q], ed[q].x);
+    push_far(P, E, to_far, ed[q].x, cand[q]);
+    t.pushes += (to_slot || to_far) ? 1 : 0;
+  }
 }
 
 // Publish `nch` hub chunks of vertex hv taken from slot s (warp-collective):
@@ -399,10 +427,11 @@ __device__ void take_entries(const AParams& P, const View& E, uint32_t s, uint32
     uint32_t v = 0;
     bool take = false;
     if (present) {
-      uint32_t* wp = slot_queue(P, s) + ((c + j0 + lane_id()) % P.cap);
-      v = wait_word(P, wp);
+      const uint32_t pos = c + j0 + lane_id();
+      unsigned long long* wp = slot_queue(P, s) + (pos % P.cap);
+      v = wait_word(P, wp, pos);
       if (v != kEmpty) {
-        __stcg(wp, kEmpty);
+        __stcg(wp, kEmpty64);
         // expand unless v waits in a lower bucket (it is expanded there with
         // its newer label); a duplicate taken after its twin expands again
         const uint32_t old = atomicCAS(&P.qb[v], gb, kNotQueued);
@@ -430,7 +459,11 @@ __device__ void take_chunk(const AParams& P, const View& E, unsigned long long p
   const uint32_t v = (uint32_t)ent;
   const uint32_t chunk = (uint32_t)(ent >> 37);
   const uint32_t s = (uint32_t)(ent >> 32) & 31u;
-  const uint32_t du = L::key(ld_keep((const typename L::T*)P.dist + v, t.keep));
+  uint32_t du = L::key(ld_keep((const typename L::T*)P.dist + v, t.keep));
+  // a label that has dropped into a lower bucket since the chunk was published
+  // is expanded from there, all its chunks included; relaxing from it here
+  // could push into a bucket below s that is already complete
+  if (du != kInfKey && slot_of<W>(E, du) < s) du = kInfKey;
   const uint64_t rb = __ldg(P.rowptr + v), re = __ldg(P.rowptr + v + 1);
   const uint64_t e0 = rb + (uint64_t)chunk * kChunkEdges;
   const uint64_t e1 = min(re, e0 + kChunkEdges);
@@ -468,11 +501,10 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
 // Claims from the shared queues go through one warp per block: it claims up
 // to kBlockClaimMax entries of a bucket (or kHubClaim hub chunks) with one
 // compare-and-swap and publishes the range in shared memory, where the
-// block's warps take kGrab entries (or one chunk) at a time with shared
-// atomics.  A ticket is (generation << 32) | next; the range of a generation
-// sits in the descriptor of its parity, tagged with the generation, so a
-// ticket from a range that has been replaced finds a stale tag and is
-// dropped.
+// block's warps take kGrab entries (or one chunk) at a time with a
+// shared-memory compare-and-swap on the range's ticket, (generation << 32) |
+// next.  The range of a generation sits in the descriptor of its parity,
+// tagged with the generation.
 struct PoolDesc {
   unsigned long long base;   // first claimed position (entries: slot position; hubs: ring position)
   uint32_t count;
@@ -502,17 +534,40 @@ __device__ __forceinline__ void publish_range(unsigned long long* ticket, PoolDe
 }
 
 // Lane 0: take up to `want` items of the block's current range.  Returns the
-// count (0: empty or stale) with the first item's position and the slot.
+// count (0: the range is used up) with the first item's position and the slot.
+// The descriptor is read between a ticket read and the compare-and-swap that
+// advances the ticket; tickets only grow, so a successful swap proves no new
+// range was published in between and the descriptor read was the ticket's.
 __device__ __forceinline__ uint32_t grab(unsigned long long* ticket, const PoolDesc* d, uint32_t want,
                                          unsigned long long* first, uint32_t* slot) {
-  const unsigned long long t = atomicAdd(ticket, (unsigned long long)want);
+  for (int tries = 0; tries < 64; ++tries) {
+    const unsigned long long t = *(volatile unsigned long long*)ticket;
+    const uint32_t g = (uint32_t)(t >> 32), i = (uint32_t)t;
+    const PoolDesc& x = d[g & 1];
+    if (*(const volatile uint32_t*)&x.gen != g) return 0;   // being published (by this block's lock holder)
+    const uint32_t cnt = *(const volatile uint32_t*)&x.count;
+    if (i >= cnt) return 0;
+    const unsigned long long base = *(const volatile unsigned long long*)&x.base;
+    const uint32_t sl = *(const volatile uint32_t*)&x.slot;
+    const uint32_t k = min(want, cnt - i);
+    if (atomicCAS(ticket, t, t + k) == t) {
+      *first = base + i;
+      *slot = sl;
+      return k;
+    }
+  }
+  return 0;
+}
+
+// Items left in the block's current range (read by the lock holder, the only
+// warp that publishes ranges).
+__device__ __forceinline__ uint32_t pool_left(const unsigned long long* ticket, const PoolDesc* d) {
+  const unsigned long long t = *(const volatile unsigned long long*)ticket;
   const uint32_t g = (uint32_t)(t >> 32), i = (uint32_t)t;
   const PoolDesc& x = d[g & 1];
+  if (*(const volatile uint32_t*)&x.gen != g) return 0;
   const uint32_t cnt = *(const volatile uint32_t*)&x.count;
-  if (*(const volatile uint32_t*)&x.gen != g || i >= cnt) return 0;
-  *first = x.base + i;
-  *slot = x.slot;
-  return min(want, cnt - i);
+  return i < cnt ? cnt - i : 0u;
 }
 
 __device__ __forceinline__ bool slot_complete(const AddsControl* c, uint32_t s);
@@ -527,6 +582,8 @@ __device__ bool refill(const AParams& P, BlockPool& sp) {
   const uint32_t pos = (uint32_t)hw;
   *(volatile uint32_t*)&sp.pos = pos;
   if (pos > (uint32_t)kAddsSlots) return false;   // a split or the end
+  // a range is replaced only once it is used up, so no claimed item is dropped
+  if (pool_left(&sp.hticket, sp.hub) || pool_left(&sp.ticket, sp.ent)) return true;
   // hub chunks
   for (int tries = 0; tries < 4; ++tries) {
     const unsigned long long cl = ld_vol64(&c->hub_claim);
@@ -820,7 +877,7 @@ __device__ void init_start(const AParams& P) {
   const uint32_t zk = P.is_float ? f32_to_key(0.0f) : 0u;
   ((typename L::T*)P.dist)[P.source] = L::make(zk, 0u);
   P.qb[P.source] = 0u;
-  slot_queue(P, 0)[0] = P.source;
+  slot_queue(P, 0)[0] = ring_word(0u, P.source);
   for (int s = 0; s < kAddsSlots; ++s) {
     c->slot[s].claim = 1ull << 32;
     c->slot[s].reserved = 0;
@@ -942,12 +999,13 @@ b2_status ensure_adds(b2_graph g, uint32_t cap_opt, cudaStream_t st) {
   Workspace& w = g->ws;
   const size_t n = (size_t)g->n;
   // a bucket ring holds the entries of its waiting vertices (at most n) plus
-  // slack for claim counts read while other blocks claim
-  const size_t full = n + std::min<size_t>(n, (size_t)1 << 19) + 1024;
+  // the claims in flight (block pools and warps: under 2^19 on a full grid);
+  // small graphs get 2^18 words so a busy bucket seldom laps its ring
+  const size_t full = std::max<size_t>(n + std::min<size_t>(n, (size_t)1 << 19), (size_t)1 << 18) + 1024;
   const size_t cap = (cap_opt > 0 && cap_opt < full) ? cap_opt : full;
   if (w.adds_q && w.adds_cap == cap) return B2_SUCCESS;
   free_adds_workspace(w);
-  cudaError_t e = cudaMalloc((void**)&w.adds_q, std::max<size_t>((size_t)(kAddsSlots + 2) * cap * 4, 16));
+  cudaError_t e = cudaMalloc((void**)&w.adds_q, (size_t)kAddsSlots * cap * 8 + (size_t)2 * cap * 4 + 16);
   // chunks waiting at once: at most two expansions' worth of every hub row
   w.adds_hub_cap = std::min<size_t>(2 * ((size_t)g->m / kChunkEdges + 1) + 65536, 0x7FFFFFFFull);
   if (e == cudaSuccess) e = cudaMalloc((void**)&w.adds_hub, w.adds_hub_cap * sizeof(unsigned long long));
@@ -1024,7 +1082,8 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   P.edges = g->edges;
   P.qb = w.adds_qb;
   P.farflag = w.farflag;
-  P.q = w.adds_q;
+  P.q = (unsigned long long*)w.adds_q;
+  P.far = (uint32_t*)((char*)w.adds_q + (size_t)kAddsSlots * w.adds_cap * 8);
   P.cap = (uint32_t)w.adds_cap;
   P.hub = (unsigned long long*)w.adds_hub;
   P.hub_cap = (uint32_t)w.adds_hub_cap;
@@ -1074,7 +1133,7 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
     stats->policy_used = policy_used;
   }
   if (w.adds_dirty) {
-    B2_CUDA_TRY(cudaMemsetAsync(w.adds_q, 0xFF, (size_t)kAddsSlots * w.adds_cap * 4, st));
+    B2_CUDA_TRY(cudaMemsetAsync(w.adds_q, 0xFF, (size_t)kAddsSlots * w.adds_cap * 8, st));
     B2_CUDA_TRY(cudaMemsetAsync(w.adds_hub, 0xFF, w.adds_hub_cap * sizeof(unsigned long long), st));
   }
   B2_CUDA_TRY(cudaMemsetAsync(w.adds_ctl, 0, sizeof(AddsControl), st));
@@ -1111,6 +1170,7 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
     stats->pushes = hc.pushes;
     stats->kernel_ms = ms;
     stats->device_error = hc.error;
+    stats->device_error_site = hc.error_site;
     stats->grid_blocks = (uint32_t)grid;
     stats->delta_updates = hc.delta_updates;
     float inv;

@@ -73,6 +73,52 @@ __device__ __forceinline__ unsigned long long atom_min_keep(unsigned long long* 
   return old;
 }
 
+// Predicated forms: the access is made only when `p` holds (the result is then
+// `dflt`), with no branch around it, so a loop can issue the accesses of all
+// its edge slots before it reads any result and their L2 round trips overlap.
+__device__ __forceinline__ uint32_t ld_keep_if(bool p, const uint32_t* a, uint64_t pol, uint32_t dflt) {
+  uint32_t v = dflt;
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t"
+               "@q ld.global.cg.L2::cache_hint.u32 %0, [%1], %2;\n\t}"
+               : "+r"(v) : "l"(a), "l"(pol), "r"((uint32_t)p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_keep_if(bool p, const unsigned long long* a, uint64_t pol,
+                                                         unsigned long long dflt) {
+  unsigned long long v = dflt;
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t"
+               "@q ld.global.cg.L2::cache_hint.u64 %0, [%1], %2;\n\t}"
+               : "+l"(v) : "l"(a), "l"(pol), "r"((uint32_t)p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t atom_min_keep_if(bool p, uint32_t* a, uint32_t x, uint64_t pol, uint32_t dflt) {
+  uint32_t old = dflt;
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %4, 0;\n\t"
+               "@q atom.global.L2::cache_hint.min.u32 %0, [%1], %2, %3;\n\t}"
+               : "+r"(old) : "l"(a), "r"(x), "l"(pol), "r"((uint32_t)p) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long atom_min_keep_if(bool p, unsigned long long* a, unsigned long long x,
+                                                               uint64_t pol, unsigned long long dflt) {
+  unsigned long long old = dflt;
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %4, 0;\n\t"
+               "@q atom.global.L2::cache_hint.min.u64 %0, [%1], %2, %3;\n\t}"
+               : "+l"(old) : "l"(a), "l"(x), "l"(pol), "r"((uint32_t)p) : "memory");
+  return old;
+}
+__device__ __forceinline__ uint32_t atom_min_if(bool p, uint32_t* a, uint32_t x, uint32_t dflt) {
+  uint32_t old = dflt;
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t@q atom.global.min.u32 %0, [%1], %2;\n\t}"
+               : "+r"(old) : "l"(a), "r"(x), "r"((uint32_t)p) : "memory");
+  return old;
+}
+__device__ __forceinline__ uint32_t atom_exch_if(bool p, uint32_t* a, uint32_t x, uint32_t dflt) {
+  uint32_t old = dflt;
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t@q atom.global.exch.b32 %0, [%1], %2;\n\t}"
+               : "+r"(old) : "l"(a), "r"(x), "r"((uint32_t)p) : "memory");
+  return old;
+}
+
 __device__ __forceinline__ uint32_t lanemask_le() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));

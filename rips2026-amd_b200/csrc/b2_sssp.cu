@@ -61,6 +61,9 @@ constexpr int kThreads = 512;
 #ifndef B2_UNROLL
 #define B2_UNROLL 4
 #endif
+#ifndef B2_SSSP_MINB      // resident blocks per SM the register budget of k_sssp is sized for
+#define B2_SSSP_MINB 2
+#endif
 #ifndef B2_HUB_UNROLL
 #define B2_HUB_UNROLL 4
 #endif
@@ -110,7 +113,6 @@ struct Params {
   uint32_t dense_min;     // delta: near / slot frontiers of at least this many entries are swept
   uint32_t qcap;          // entries each worklist queue may hold (<= n; a push past it is kErrQueueOverflow)
   ProgressBoard* board;   // mapped progress record (null: no progress callback)
-  uint32_t small_items;   // queue items shrink below 32 vertices for small frontiers
 };
 
 // Bucket of a distance key under the phase's mapping
@@ -336,9 +338,84 @@ __device__ __forceinline__ void route(const Params& P, const PhaseRec& R, bool i
   }
 }
 
-// Relax U edge slots per lane: loads first, then atomics, then routing.
-// Staged pushes are flushed after every kUnroll routed slots, so a warp
-// buffer never takes more than kUnroll x 32 entries past its flush mark.
+// Route the improvements of U edge slots per lane (warp-collective).  The
+// dedup atomics of every slot go out before any result is read, so their
+// round trips overlap; then each slot is staged in order.  Staged pushes are
+// flushed after every kUnroll slots, so a warp buffer never takes more than
+// kUnroll x 32 entries past its flush mark.
+template <class W, int MODE, int U>
+__device__ __forceinline__ void route_batch(const Params& P, const PhaseRec& R, const bool (&imp)[U],
+                                            const uint2 (&ed)[U], const uint32_t (&cand)[U], Tally& t) {
+  bool any_imp = false;
+#pragma unroll
+  for (int q = 0; q < U; ++q) any_imp = any_imp || imp[q];
+  if (!__any_sync(0xffffffffu, any_imp)) return;
+  Control* c = P.ctl;
+  uint32_t b[U], onear[U], obuck[U];
+  int cls[U];   // 0 none, 1 near, 2 window slot, 3 far
+#pragma unroll
+  for (int q = 0; q < U; ++q) {
+    b[q] = 0;
+    cls[q] = 0;
+    if (imp[q]) {
+      if (MODE == kModeBF) {
+        cls[q] = 1;
+      } else {
+        b[q] = bucket_of<W>(R, cand[q]);
+        cls[q] = b[q] <= R.cur ? 1 : (b[q] < R.win + (uint32_t)kRing ? 2 : 3);
+      }
+    }
+    // defaults read as "already queued"
+    onear[q] = atom_exch_if(cls[q] == 1, &P.pstamp[ed[q].x], R.stamp, R.stamp);
+    obuck[q] = MODE == kModeBF ? 0u : atom_min_if(cls[q] >= 2, &P.bstamp[ed[q].x], b[q], 0u);
+  }
+  uint32_t ofar[U];
+  bool any_far = false;
+#pragma unroll
+  for (int q = 0; q < U; ++q) {
+    const bool f = MODE != kModeBF && cls[q] == 3 && obuck[q] > b[q];
+    any_far = any_far || f;
+    ofar[q] = f ? 0u : 1u;
+  }
+  if (MODE != kModeBF && any_far) {
+#pragma unroll
+    for (int q = 0; q < U; ++q) ofar[q] = atom_exch_if(ofar[q] == 0u, &P.farflag[ed[q].x], 1u, 1u);
+  }
+#pragma unroll
+  for (int q = 0; q < U; ++q) {
+    const uint32_t v = ed[q].x;
+    if (__any_sync(0xffffffffu, cls[q] == 1)) {
+      const bool want = cls[q] == 1 && onear[q] != R.stamp;
+      stage(t.q.nearb, t.q.nn, want, v);
+      t.pushes += want ? 1 : 0;
+    }
+    if (MODE != kModeBF) {
+      if (__any_sync(0xffffffffu, cls[q] == 2)) {
+        const bool want = cls[q] == 2 && obuck[q] > b[q];
+        const uint32_t bal = __ballot_sync(0xffffffffu, want);
+        if (want) {
+          const uint32_t pos = t.q.ns + __popc(bal & ((1u << lane_id()) - 1u));
+          t.q.slotb[2 * pos] = v;
+          t.q.slotb[2 * pos + 1] = b[q] - R.win;
+        }
+        t.q.ns += __popc(bal);
+        t.pushes += want ? 1 : 0;
+      }
+      if (__any_sync(0xffffffffu, cls[q] == 3)) {
+        const bool lowered = cls[q] == 3 && obuck[q] > b[q];
+        const bool want = lowered && ofar[q] == 0u;
+        const uint32_t bmin = __reduce_min_sync(0xffffffffu, lowered ? b[q] : 0xFFFFFFFFu);
+        if (lane_id() == 0 && bmin != 0xFFFFFFFFu) atomicMin(&c->far_min, bmin);
+        stage(t.q.farb, t.q.nf, want, v);
+        t.pushes += want ? 1 : 0;
+      }
+    }
+    if ((q % kUnroll) == kUnroll - 1) flush_all<MODE>(P, R, t.q, false);
+  }
+}
+
+// Relax U edge slots per lane: label loads first, then the atomics of every
+// slot (issued before any result is read), then routing.
 template <class W, bool PRED, int MODE, int U>
 __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, const bool (&act)[U],
                                             const uint32_t (&src)[U], const uint32_t (&dsrc)[U],
@@ -346,33 +423,28 @@ __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, 
   using L = Label<PRED>;
   typename L::T* lab = (typename L::T*)P.dist;
   uint32_t cand[U];
-  typename L::T cur[U];
+  typename L::T cur[U], old[U];
   bool imp[U];
 #pragma unroll
   for (int q = 0; q < U; ++q) {
     cand[q] = act[q] ? W::extend(dsrc[q], ed[q].y) : kInfKey;
-    cur[q] = (cand[q] != kInfKey) ? ld_keep(lab + ed[q].x, t.keep) : L::kInf;
+    cur[q] = ld_keep_if(cand[q] != kInfKey, lab + ed[q].x, t.keep, L::kInf);
   }
 #pragma unroll
   for (int q = 0; q < U; ++q) {
-    imp[q] = false;
-    if (cand[q] != kInfKey) {
-      const typename L::T cw = L::make(cand[q], src[q]);
-      if (cw < cur[q]) {
-        const typename L::T old = atom_min_keep(lab + ed[q].x, cw, t.keep);
-        // (PRED: a smaller predecessor at an equal distance updates the word
-        //  but does not re-expand the vertex.)
-        imp[q] = cand[q] < L::key(old);
-      }
-    }
+    const typename L::T cw = L::make(cand[q], src[q]);
+    // not issued: old = 0 reads as "no improvement"
+    old[q] = atom_min_keep_if(cand[q] != kInfKey && cw < cur[q], lab + ed[q].x, cw, t.keep, (typename L::T)0);
+  }
+#pragma unroll
+  for (int q = 0; q < U; ++q) {
+    // (PRED: a smaller predecessor at an equal distance updates the word
+    //  but does not re-expand the vertex.)
+    imp[q] = cand[q] < L::key(old[q]);
     t.edges += act[q] ? 1 : 0;
     t.impr += imp[q] ? 1 : 0;
   }
-#pragma unroll
-  for (int q = 0; q < U; ++q) {
-    route<W, MODE>(P, R, imp[q], ed[q].x, cand[q], t);
-    if ((q % kUnroll) == kUnroll - 1) flush_all<MODE>(P, R, t.q, false);
-  }
+  route_batch<W, MODE, U>(P, R, imp, ed, cand, t);
 }
 
 template <class W, bool PRED, int MODE>
@@ -645,7 +717,7 @@ __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t g = 32;
-  if (!dense && P.small_items)
+  if (!dense)
     while (g > 1 && (R.fcount + g - 1) / g < nwarps) g >>= 1;
   const uint32_t nfc = dense ? (P.n + kDenseSpan - 1) / kDenseSpan : (R.fcount + g - 1) / g;
   const uint32_t items = nhg + nfc;
@@ -1171,7 +1243,7 @@ __device__ void local_phase(const Params& P, const PhaseRec& R0, Tally& t) {
 
 // ---------------------------------------------------------------------------
 template <class W, bool PRED, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) k_sssp(Params P) {
+__global__ void __launch_bounds__(kThreads, B2_SSSP_MINB) k_sssp(Params P) {
   using L = Label<PRED>;
   __shared__ PhaseRec s_rec;
   extern __shared__ uint32_t s_stage[];   // kStageWords per warp
@@ -1518,7 +1590,6 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
   memset(&P, 0, sizeof(P));
   P.n = (uint32_t)g->n;
   P.qcap = (o.worklist_capacity > 0 && (int64_t)o.worklist_capacity < g->n) ? o.worklist_capacity : P.n;
-  P.small_items = std::getenv("B2_ITEM32") ? 0u : 1u;
   P.source = internal_id(g, source);
   P.perm = g->perm;
   P.inv = g->perm ? g->inv : nullptr;
@@ -1677,6 +1748,7 @@ b2_status run_sssp(b2_graph g, int mode, uint32_t source, void* d_dist, int32_t*
     stats->pushes = hc.pushes;
     stats->kernel_ms = ms;
     stats->device_error = hc.error;
+    stats->device_error_site = hc.error_site;
     stats->grid_blocks = (uint32_t)grid;
     stats->first_unchanged = hc.first_unchanged;
     stats->local_subphases = hc.local_total;

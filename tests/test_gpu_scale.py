@@ -101,13 +101,15 @@ def test_budget_runs_out_then_next_solve_is_exact(b2, orc, cuda, method):
 def test_worklist_capacity_overflow_is_pool_exhausted(b2, orc, cuda, method):
     from b200sssp import _lib
     hg = b2.gen_rmat(16, 16, 0.57, 0.19, 0.19, 1, 255, 9)
+    src = int(np.argmax(np.diff(hg.rowptr)))   # the largest hub: its first frontier alone passes 64
     g = b2.Graph.from_host(hg, "u32")
     with pytest.raises(_lib.B2Error) as ei:
-        g.sssp(1, method=method, worklist_capacity=64)
+        g.sssp(src, method=method, worklist_capacity=64)
     assert ei.value.status == _lib.POOL_EXHAUSTED
-    d, _, _ = g.sssp(1, method=method)
-    assert np.array_equal(_u32(d), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 1))
+    ref = orc.dijkstra(hg.rowptr, hg.colind, hg.weights, src)
+    d, _, _ = g.sssp(src, method=method)
+    assert np.array_equal(_u32(d), ref)
     # a capacity the solve never reaches changes nothing
-    d, _, _ = g.sssp(1, method=method, worklist_capacity=hg.n - 1)
-    assert np.array_equal(_u32(d), orc.dijkstra(hg.rowptr, hg.colind, hg.weights, 1))
+    d, _, _ = g.sssp(src, method=method, worklist_capacity=hg.n - 1)
+    assert np.array_equal(_u32(d), ref)
     g.close()
