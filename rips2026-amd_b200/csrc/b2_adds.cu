@@ -45,8 +45,8 @@
 // side, so an improvement is never left unexpanded.
 //
 // High-degree vertices are split into chunks of kChunkEdges edges in a ring
-// that any warp may take (counted in their bucket's `extra` before they are
-// published).  Labels and relaxation are those of the bulk-synchronous kernel
+// of position-tagged slots that any warp may take (counted in their bucket's
+// `extra` before they are published).  Labels and relaxation are those of the bulk-synchronous kernel
 // (b2_relax.cuh): 32-bit keys or packed key|pred words, one hardware atomicMin.
 // Every wait is bounded by the solve budget; on expiry the kernel records
 // kErrTimeout and every warp leaves.
@@ -86,7 +86,7 @@ struct AParams {
   unsigned long long* q;   // kAddsSlots window rings of cap tagged words (position << 32 | vertex)
   uint32_t* far;           // the two far piles, cap entries each
   uint32_t cap;
-  unsigned long long* hub; // ring of {v, chunk << 5 | slot}
+  ulonglong2* hub;         // ring of {position tag, v | (chunk << 5 | slot) << 32}; tag ~0: empty
   uint32_t hub_cap;
   AddsControl* ctl;
   TraceEntry* trace;
@@ -121,6 +121,15 @@ struct ATally {
 __device__ __forceinline__ uint32_t ld_vol(const uint32_t* p) { return *(const volatile uint32_t*)p; }
 __device__ __forceinline__ unsigned long long ld_vol64(const unsigned long long* p) {
   return *(const volatile unsigned long long*)p;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ void set_err(const AParams& P, uint32_t code, uint32_t site) {
@@ -189,14 +198,14 @@ __device__ uint32_t wait_word(const AParams& P, const unsigned long long* p, uin
     }
   }
 }
-__device__ unsigned long long wait_hub(const AParams& P, const unsigned long long* p) {
-  unsigned long long v = ld_vol64(p);
-  if (v != kEmpty64) return v;
+// Bounded wait for the hub chunk of ring position `pos`: its tag is stored
+// (release) after its entry, so an acquire of the tag makes the entry
+// readable.  Returns the entry (kEmpty64: the wait gave up).
+__device__ unsigned long long wait_hub(const AParams& P, ulonglong2* slot, unsigned long long pos) {
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 0;; ++i) {
+    if (ld_acquire_u64(&slot->x) == pos) return ld_vol64(&slot->y);
     __nanosleep(32);
-    v = ld_vol64(p);
-    if (v != kEmpty64) return v;
     if ((i & 63u) == 63u) {
       if (ld_vol(&P.ctl->error)) return kEmpty64;
       if (globaltimer_ns() - t0 > P.budget_ns) {
@@ -327,7 +336,9 @@ __device__ __forceinline__ void relax_route(const AParams& P, const View& E, con
 }
 
 // Publish `nch` hub chunks of vertex hv taken from slot s (warp-collective):
-// the bucket's `extra` grows before any chunk becomes visible.
+// the bucket's `extra` grows before any chunk becomes visible.  Ring position
+// p lives at p % hub_cap; its writer waits (bounded) until the chunk of the
+// previous lap there has been taken, then stores the entry and, last, the tag.
 __device__ __forceinline__ void publish_hub(const AParams& P, uint32_t hv, uint32_t nch, uint32_t s) {
   unsigned long long hb = 0;
   if (lane_id() == 0) {
@@ -337,12 +348,23 @@ __device__ __forceinline__ void publish_hub(const AParams& P, uint32_t hv, uint3
   }
   hb = shfl64(hb, 0);
   for (uint32_t j = lane_id(); j < nch; j += 32) {
-    unsigned long long* e = P.hub + (size_t)((hb + j) % P.hub_cap);
-    if (ld_vol64(e) != kEmpty64) {   // the ring is full: an older chunk is still waiting here
-      set_err(P, kErrQueueOverflow, 44);
-    } else {
-      *(volatile unsigned long long*)e = ((unsigned long long)((j << 5) | s) << 32) | hv;
+    ulonglong2* e = P.hub + (size_t)((hb + j) % P.hub_cap);
+    if (ld_vol64(&e->x) != kEmpty64) {
+      const uint64_t t0 = globaltimer_ns();
+      bool gave_up = false;
+      while (ld_vol64(&e->x) != kEmpty64) {
+        __nanosleep(64);
+        if (ld_vol(&P.ctl->error)) { gave_up = true; break; }
+        if (globaltimer_ns() - t0 > P.budget_ns) {
+          set_err(P, kErrTimeout, 44);
+          gave_up = true;
+          break;
+        }
+      }
+      if (gave_up) continue;
     }
+    *(volatile unsigned long long*)&e->y = ((unsigned long long)((j << 5) | s) << 32) | hv;
+    st_release_u64(&e->x, hb + j);
   }
 }
 
@@ -450,9 +472,9 @@ __device__ void take_chunk(const AParams& P, const View& E, unsigned long long p
   using L = Label<PRED>;
   unsigned long long ent = 0;
   if (lane_id() == 0) {
-    unsigned long long* e = P.hub + (size_t)(pos % P.hub_cap);
-    ent = wait_hub(P, e);
-    if (ent != kEmpty64) *(volatile unsigned long long*)e = kEmpty64;
+    ulonglong2* e = P.hub + (size_t)(pos % P.hub_cap);
+    ent = wait_hub(P, e, pos);
+    if (ent != kEmpty64) st_release_u64(&e->x, kEmpty64);   // after the entry was read
   }
   ent = shfl64(ent, 0);
   if (ent == kEmpty64) return;   // the wait gave up (error recorded)
@@ -488,15 +510,6 @@ __device__ void take_chunk(const AParams& P, const View& E, unsigned long long p
 __device__ __forceinline__ unsigned long long head_word(uint32_t epoch, uint32_t pos) {
   return ((unsigned long long)epoch << 32) | pos;
 }
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
 // ---- per-block work pools --------------------------------------------------
 // Claims from the shared queues go through one warp per block: it claims up
 // to kBlockClaimMax entries of a bucket (or kHubClaim hub chunks) with one
@@ -519,6 +532,7 @@ struct BlockPool {
   PoolDesc hub[2];
   uint32_t lock;
   uint32_t pos;                // head position the refilling warp saw last
+  View view;                   // the epoch of the ranges published here (set before the first one)
 };
 
 __device__ __forceinline__ void publish_range(unsigned long long* ticket, PoolDesc* d, unsigned long long base,
@@ -584,6 +598,17 @@ __device__ bool refill(const AParams& P, BlockPool& sp) {
   if (pos > (uint32_t)kAddsSlots) return false;   // a split or the end
   // a range is replaced only once it is used up, so no claimed item is dropped
   if (pool_left(&sp.hticket, sp.hub) || pool_left(&sp.ticket, sp.ent)) return true;
+  // the block's copy of the epoch view: a claimed unit pins its epoch, so the
+  // view stays right while any warp of the block holds one
+  const uint32_t ep = (uint32_t)(hw >> 32);
+  if (*(volatile uint32_t*)&sp.view.epoch != ep) {
+    const View E = read_view(c);
+    if (E.epoch != ep) return false;   // the head moved on meanwhile
+    volatile uint32_t* dv = (volatile uint32_t*)&sp.view;
+    const uint32_t* sv = (const uint32_t*)&E;
+    for (int i = 0; i < (int)(sizeof(View) / 4); ++i) dv[i] = sv[i];
+    __threadfence_block();
+  }
   // hub chunks
   for (int tries = 0; tries < 4; ++tries) {
     const unsigned long long cl = ld_vol64(&c->hub_claim);
@@ -809,15 +834,19 @@ __device__ void idle_step(const AParams& P) {
 template <class W, bool PRED>
 __device__ void worker(const AParams& P, BlockPool& sp, ATally& t) {
   AddsControl* c = P.ctl;
-  uint32_t idle = 0;
+  uint32_t idle = 0, iter = 0;
+  const unsigned long long t_start = ld_vol64(&c->t_start);
   for (;;) {
     uint32_t pos = 0, err = 0;
     if (lane_id() == 0) {
       pos = *(volatile uint32_t*)&sp.pos;
-      err = ld_vol(&c->error);
-      if (!err && globaltimer_ns() - ld_vol64(&c->t_start) > P.budget_ns) {
-        set_err(P, kErrTimeout, 45);
-        err = 1;
+      // the error flag and the budget every 8th pass (every wait checks them too)
+      if ((++iter & 7u) == 0u || idle) {
+        err = ld_vol(&c->error);
+        if (!err && globaltimer_ns() - t_start > P.budget_ns) {
+          set_err(P, kErrTimeout, 45);
+          err = 1;
+        }
       }
     }
     pos = __shfl_sync(kFull, pos, 0);
@@ -848,10 +877,14 @@ __device__ void worker(const AParams& P, BlockPool& sp, ATally& t) {
       first = shfl64(first, 0);
       k = __shfl_sync(kFull, k, 0);
       slot = __shfl_sync(kFull, slot, 0);
-      // a claimed unit pins its epoch (its bucket cannot complete): read it now
+      // a claimed unit pins its epoch (its bucket cannot complete), so the
+      // block's view, set before the range was published, is its epoch's
       View E;
-      if (lane_id() == 0) E = read_view(c);
-      E = bcast(E);
+      {
+        const volatile uint32_t* sv = (const volatile uint32_t*)&sp.view;
+        uint32_t* dv = (uint32_t*)&E;
+        for (int i = 0; i < (int)(sizeof(View) / 4); ++i) dv[i] = sv[i];
+      }
       if (kind == 1) take_chunk<W, PRED>(P, E, first, t);
       else take_entries<W, PRED>(P, E, slot, (uint32_t)first, k, t);
       idle = 0;
@@ -1007,8 +1040,8 @@ b2_status ensure_adds(b2_graph g, uint32_t cap_opt, cudaStream_t st) {
   free_adds_workspace(w);
   cudaError_t e = cudaMalloc((void**)&w.adds_q, (size_t)kAddsSlots * cap * 8 + (size_t)2 * cap * 4 + 16);
   // chunks waiting at once: at most two expansions' worth of every hub row
-  w.adds_hub_cap = std::min<size_t>(2 * ((size_t)g->m / kChunkEdges + 1) + 65536, 0x7FFFFFFFull);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&w.adds_hub, w.adds_hub_cap * sizeof(unsigned long long));
+  w.adds_hub_cap = std::min<size_t>(4 * ((size_t)g->m / kChunkEdges + 1) + 65536, 0x7FFFFFFFull);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&w.adds_hub, w.adds_hub_cap * sizeof(ulonglong2));
   if (e == cudaSuccess) e = cudaMalloc((void**)&w.adds_qb, std::max<size_t>(n * 4, 16));
   if (e == cudaSuccess) e = cudaMalloc((void**)&w.adds_ctl, sizeof(AddsControl));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&w.adds_h_ctl, sizeof(AddsControl));
@@ -1085,7 +1118,7 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   P.q = (unsigned long long*)w.adds_q;
   P.far = (uint32_t*)((char*)w.adds_q + (size_t)kAddsSlots * w.adds_cap * 8);
   P.cap = (uint32_t)w.adds_cap;
-  P.hub = (unsigned long long*)w.adds_hub;
+  P.hub = (ulonglong2*)w.adds_hub;
   P.hub_cap = (uint32_t)w.adds_hub_cap;
   P.ctl = w.adds_ctl;
   P.trace = o.trace ? w.trace : nullptr;
@@ -1134,7 +1167,7 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   }
   if (w.adds_dirty) {
     B2_CUDA_TRY(cudaMemsetAsync(w.adds_q, 0xFF, (size_t)kAddsSlots * w.adds_cap * 8, st));
-    B2_CUDA_TRY(cudaMemsetAsync(w.adds_hub, 0xFF, w.adds_hub_cap * sizeof(unsigned long long), st));
+    B2_CUDA_TRY(cudaMemsetAsync(w.adds_hub, 0xFF, w.adds_hub_cap * sizeof(ulonglong2), st));
   }
   B2_CUDA_TRY(cudaMemsetAsync(w.adds_ctl, 0, sizeof(AddsControl), st));
   s = progress_begin(g, o, &P.board);

@@ -262,7 +262,7 @@ struct Workspace {
   // ADDS worklist (allocated on the first b2_sssp_adds solve)
   void* adds_q = nullptr;           // kAddsSlots rings of adds_cap 64-bit words, then 2 far piles of adds_cap u32
   size_t adds_cap = 0;
-  uint2* adds_hub = nullptr;        // ring of hub chunks {v, chunk << 5 | slot}
+  void* adds_hub = nullptr;         // ring of 16-byte hub-chunk slots {position tag, entry}
   size_t adds_hub_cap = 0;
   uint32_t* adds_qb = nullptr;      // per vertex: global bucket it is queued in (unprocessed), else ~0
   AddsControl* adds_ctl = nullptr;

@@ -14,6 +14,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "rips2026-amd_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# a solve that has not finished in 10 s has gone wrong: fail it on the device
+# (bounded waits return B2_TIMEOUT) instead of waiting out the 20 s default
+os.environ.setdefault("B2_TIMEOUT_MS", "10000")
 
 
 def pytest_configure(config):
