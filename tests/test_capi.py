@@ -34,7 +34,9 @@ def test_status_strings_and_defaults(b2):
     assert _lib.lib().b2_abi_version() == 1
     for s in range(12):
         assert _lib.status_string(s) and "unknown" not in _lib.status_string(s)
-    o = _lib.default_opts()
+    import ctypes
+    o = _lib.Opts()   # the library's own defaults (default_opts() also applies B2_TIMEOUT_MS)
+    _lib.lib().b2_sssp_opts_default(ctypes.byref(o))
     assert o.max_iters == -1 and o.delta_scale == 16.0 and o.timeout_ms == 20000.0 and o.hub_degree == 256
     assert o.pull_fraction == 8.0 and o.dense_fraction == 0.0 and o.light_heavy == 1   # 0: by graph degree
 
