@@ -184,7 +184,11 @@ typedef struct b2_sssp_opts {
   b2_progress_fn progress;  /* nullable: called once per finished round / bucket, in order,
                                while the solve runs (every call precedes the return) */
   void* progress_user;
-  int32_t reserved[3];
+  uint32_t max_active_buckets; /* ADDS: the active range never widens past this many buckets
+                               (0: 32, the whole window; hip_adds::Options::max_active_buckets,
+                               hip_adds_sssp.hpp:37-38).  Equal to active_buckets: no widening
+                               (the reference's dynamic_active_buckets = false). */
+  int32_t reserved[2];
 } b2_sssp_opts;
 
 typedef struct b2_trace_entry {

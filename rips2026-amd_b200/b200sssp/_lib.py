@@ -54,7 +54,8 @@ class Opts(C.Structure):
                 ("detect_negative_cycle", C.c_int32), ("light_heavy", C.c_int32), ("trace", C.c_int32),
                 ("dense_fraction", C.c_float), ("worklist_capacity", C.c_uint32), ("keep_distances", C.c_int32),
                 ("active_buckets", C.c_uint32), ("adds_fixed_delta", C.c_int32), ("progress", C.c_void_p),
-                ("progress_user", C.c_void_p), ("reserved", C.c_int32 * 3)]
+                ("progress_user", C.c_void_p), ("max_active_buckets", C.c_uint32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class Progress(C.Structure):

@@ -94,6 +94,7 @@ struct AParams {
   uint32_t width_u;        // initial bucket width (uint32 graphs)
   float inv_width;         // 1 / initial width (float graphs)
   uint32_t active0;        // buckets from the head warps may take at the start of an epoch
+  uint32_t active_max;     // the active range never widens past this
   uint32_t hub_degree;
   uint32_t adapt;          // adjust the width at every new epoch
   uint32_t adapt_cap;      // entries per bucket that fill the grid once
@@ -822,7 +823,7 @@ __device__ void idle_step(const AParams& P) {
   // later buckets hold work while the active ones have none to give: widen
   const uint32_t a = ld_vol(&c->active);
   const uint32_t epoch = (uint32_t)(hw >> 32);
-  for (uint32_t j = a; j < a + 2 && h + j < (uint32_t)kAddsSlots; ++j) {
+  for (uint32_t j = a; j < a + 2 && j < P.active_max && h + j < (uint32_t)kAddsSlots; ++j) {
     if (claimable(c, h + j, epoch)) {
       atomicMax(&c->active, j + 1);
       atomicMax(&c->max_active, j + 1);
@@ -1125,6 +1126,8 @@ b2_status run_adds(b2_graph g, uint32_t source, void* d_dist, int32_t* d_pred, c
   P.is_float = isf ? 1u : 0u;
   P.hub_degree = std::max<uint32_t>(64u, o.hub_degree ? o.hub_degree : 512u);
   P.active0 = o.active_buckets > 0 ? std::min<uint32_t>(o.active_buckets, kAddsSlots) : 2u;
+  P.active_max = o.max_active_buckets > 0 ? std::min<uint32_t>(o.max_active_buckets, kAddsSlots) : (uint32_t)kAddsSlots;
+  P.active_max = std::max(P.active_max, P.active0);
   P.adapt = o.adds_fixed_delta ? 0u : 1u;
   P.budget_ns = (unsigned long long)(std::max(0.001, o.timeout_ms > 0 ? o.timeout_ms : 20000.0) * 1.0e6);
   P.out_dist = d_dist;

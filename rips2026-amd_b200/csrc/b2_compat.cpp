@@ -701,6 +701,8 @@ Status run(const DeviceCsrGraph<Weight>& graph, uint32_t source, Weight* d_dista
   o.keep_distances = options.initialize_distances ? 0 : 1;   // warm start (hip_adds_sssp.hpp:64-66)
   o.adds_fixed_delta = options.dynamic_delta ? 0 : 1;
   o.active_buckets = options.initial_active_buckets;
+  o.max_active_buckets = options.dynamic_active_buckets ? options.max_active_buckets
+                                                        : std::max<uint32_t>(1u, options.initial_active_buckets);
   if (options.worker_blocks) o.grid_blocks = options.worker_blocks;
   // pool_words is the reference's whole worklist pool; here each of the
   // window queues and far piles holds an equal share

@@ -40,7 +40,8 @@ def test_adds_exact_with_pred(b2, orc, cuda, weight):
 
 
 @pytest.mark.parametrize("opts", [{"delta": 1.0}, {"delta": 3.0, "adds_fixed_delta": 1}, {"active_buckets": 1},
-                                  {"active_buckets": 32}, {"hub_degree": 64}, {"grid_blocks": 7}])
+                                  {"active_buckets": 32}, {"hub_degree": 64}, {"grid_blocks": 7},
+                                  {"active_buckets": 1, "max_active_buckets": 1}, {"max_active_buckets": 4}])
 def test_adds_schedule_options_keep_words(b2, orc, cuda, opts):
     hg = b2.gen_rmat(14, 16, seed=64)
     g = b2.Graph.from_host(hg, "u32")
@@ -51,6 +52,8 @@ def test_adds_schedule_options_keep_words(b2, orc, cuda, opts):
         assert st["phases"] > 1 and st["delta_updates"] > 0 and st["delta_final"] > 1.0
     if opts.get("adds_fixed_delta"):
         assert st["delta_updates"] == 0 and st["delta_final"] == 3.0
+    if opts.get("max_active_buckets"):
+        assert st["active_buckets_max"] <= opts["max_active_buckets"]
     g.close()
 
 
