@@ -358,6 +358,10 @@ b2_status b2_policy_get_params(b2_policy p, float* params, float* mu, float* sig
  * log2_dead_zone (chosen by cross-validation when the weights are trained;
  * stored in the weight file).  Default 0. */
 b2_status b2_policy_set_dead_zone(b2_policy p, float log2_dead_zone);
+/* Clamp each raw feature to [lo[k], hi[k]] before it is normalized (the range
+   of the training graphs; training sets it from its X).  lo = hi = NULL: no
+   clamping. */
+b2_status b2_policy_set_feature_range(b2_policy p, const float* lo, const float* hi);
 /* X: B x 24 raw features; Y: B x 3 outputs. */
 b2_status b2_policy_forward(b2_policy p, const float* X, int32_t B, float* Y);
 /* Gradient of the mean loss (y0-t0)^2 + BCE(y1,t1) + BCE(y2,t2) over the

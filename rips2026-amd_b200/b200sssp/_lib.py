@@ -131,6 +131,7 @@ _SIGS = {
     "b2_policy_set_params": (C.c_int, [_P, _P, _P, _P]),
     "b2_policy_get_params": (C.c_int, [_P, _P, _P, _P]),
     "b2_policy_set_dead_zone": (C.c_int, [_P, C.c_float]),
+    "b2_policy_set_feature_range": (C.c_int, [_P, _P, _P]),
     "b2_policy_forward": (C.c_int, [_P, _P, C.c_int32, _P]),
     "b2_policy_gradient": (C.c_int, [_P, _P, _P, C.c_int32, _P, C.POINTER(C.c_float)]),
     "b2_policy_train": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float,

@@ -114,7 +114,19 @@ class Policy:
         p = cls(0)
         p.set_params(w["params"], w["mu"], w["sigma"])
         p.set_dead_zone(float(w["dead_zone"]) if "dead_zone" in w else 0.0)
+        if "train_X" in w:   # score graphs past the training sizes like the nearest training graphs
+            X = np.asarray(w["train_X"], np.float32)
+            p.set_feature_range(X.min(axis=0), X.max(axis=0))
         return p
+
+    def set_feature_range(self, lo, hi) -> None:
+        """Clamp raw features to [lo, hi] before normalizing (None, None: no clamp)."""
+        if lo is None:
+            check(lib().b2_policy_set_feature_range(self._h, None, None), "policy_set_feature_range")
+            return
+        lo = np.ascontiguousarray(lo, np.float32)
+        hi = np.ascontiguousarray(hi, np.float32)
+        check(lib().b2_policy_set_feature_range(self._h, _fp(lo), _fp(hi)), "policy_set_feature_range")
 
     def set_dead_zone(self, log2_dead_zone: float) -> None:
         """Keep the Near-Far delta when |predicted log2 multiplier| is below this."""

@@ -181,6 +181,12 @@ struct PolicyState {
   float* grad = nullptr;
   float mu[kIn];
   float sigma[kIn];
+  // raw features are clamped to the range seen in training before they are
+  // normalized, so a graph past the training sizes is scored like the
+  // nearest training graphs rather than extrapolated
+  float lo[kIn];
+  float hi[kIn];
+  int has_range = 0;
   float dead_zone = 0.0f;   // |predicted log2 delta multiplier| below this keeps the Near-Far delta
   int step = 0;
 };
@@ -207,7 +213,11 @@ b2_status upload_params(b2_policy p, const float* host) {
 
 void normalize(const b2_policy p, const float* raw, float* out, int B) {
   for (int s = 0; s < B; ++s)
-    for (int k = 0; k < kIn; ++k) out[s * kIn + k] = (raw[s * kIn + k] - p->s.mu[k]) / p->s.sigma[k];
+    for (int k = 0; k < kIn; ++k) {
+      float x = raw[s * kIn + k];
+      if (p->s.has_range) x = std::min(std::max(x, p->s.lo[k]), p->s.hi[k]);
+      out[s * kIn + k] = (x - p->s.mu[k]) / p->s.sigma[k];
+    }
 }
 
 constexpr int kSample = 65536;
@@ -415,6 +425,22 @@ extern "C" b2_status b2_policy_set_params(b2_policy p, const float* params, cons
   return upload_params(p, params);
 }
 
+// Range of the raw features seen in training (lo/hi null: no clamping).
+extern "C" b2_status b2_policy_set_feature_range(b2_policy p, const float* lo, const float* hi) {
+  if (!p || (!lo) != (!hi)) return B2_INVALID_ARGUMENT;
+  if (lo)
+    for (int k = 0; k < kIn; ++k)
+      if (!(lo[k] <= hi[k])) return B2_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_pol_mu);
+  if (lo) {
+    memcpy(p->s.lo, lo, sizeof(p->s.lo));
+    memcpy(p->s.hi, hi, sizeof(p->s.hi));
+  }
+  p->s.has_range = lo ? 1 : 0;
+  ++g_generation;
+  return B2_SUCCESS;
+}
+
 extern "C" b2_status b2_policy_set_dead_zone(b2_policy p, float log2_dead_zone) {
   if (!p || !(log2_dead_zone >= 0.0f)) return B2_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(g_pol_mu);
@@ -487,13 +513,21 @@ extern "C" b2_status b2_policy_train(b2_policy p, const float* X, const float* T
   if (p->s.step == 0) {
     for (int k = 0; k < kIn; ++k) {
       double m = 0, v = 0;
-      for (int s = 0; s < B; ++s) m += X[s * kIn + k];
+      float lo = X[k], hi = X[k];
+      for (int s = 0; s < B; ++s) {
+        m += X[s * kIn + k];
+        lo = std::min(lo, X[s * kIn + k]);
+        hi = std::max(hi, X[s * kIn + k]);
+      }
       m /= B;
       for (int s = 0; s < B; ++s) v += (X[s * kIn + k] - m) * (X[s * kIn + k] - m);
       v /= B;
       p->s.mu[k] = (float)m;
       p->s.sigma[k] = v > 1e-12 ? (float)std::sqrt(v) : 1.0f;
+      p->s.lo[k] = lo;
+      p->s.hi[k] = hi;
     }
+    p->s.has_range = 1;
   }
   std::vector<float> xn((size_t)B * kIn);
   normalize(p, X, xn.data(), B);

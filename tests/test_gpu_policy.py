@@ -28,6 +28,27 @@ def test_forward_matches_fp64_oracle(pol, orc):
     assert np.allclose(Y, ref, rtol=1e-4, atol=1e-4)     # FP32 accumulation vs FP64
 
 
+def test_features_past_the_training_range_are_clamped(pol, orc):
+    """Raw features outside the range set by training (or from the weight file)
+    score like the nearest in-range features; clearing the range restores plain
+    normalization."""
+    p = pol.Policy(seed=5)
+    rng = np.random.default_rng(1)
+    X = rng.normal(size=(64, 24)).astype(np.float32)
+    T = rng.normal(size=(64, 3)).astype(np.float32)
+    p.train(X, T, epochs=5)                          # first training call sets the range from X
+    lo, hi = X.min(axis=0), X.max(axis=0)
+    Xo = (X[:8] * 4.0).astype(np.float32)            # mostly past the range
+    assert np.array_equal(p.forward(Xo), p.forward(np.clip(Xo, lo, hi)))
+    p.set_feature_range(None, None)
+    P, mu, sg = p.params()
+    ref = orc.mlp_forward(_bf16_params(P, orc), (Xo.astype(np.float64) - mu) / sg)
+    assert np.allclose(p.forward(Xo), ref, rtol=1e-4, atol=1e-4)
+    p.set_feature_range(lo, hi)
+    assert np.array_equal(p.forward(Xo), p.forward(np.clip(Xo, lo, hi)))
+    p.close()
+
+
 def test_gradient_matches_fp64_oracle(pol, orc):
     p = pol.Policy(seed=5)
     rng = np.random.default_rng(1)
