@@ -487,10 +487,13 @@ def _graph_line(g, sources, args, rp, ci, w, weight, kind, method="delta", opts=
     wt = "WF32" if weight == "f32" else "WU32"
     out = {"gteps": run["edges"] / run["t_dev"] / 1e9, "ms_per_solve": run["t_dev"] / args.steps * 1e3,
            "roofline": roofline(run["bytes_alg"] / args.steps, float(np.mean(run["kernel_ms"])) / 1e3,
-                                f"k_sssp<{wt},false,kModeDelta>", profile_traffic(kind) if weight == "u32" and
-                                method == "delta" else None),
+                                f"k_adds<{wt},false>" if method == "adds" else f"k_sssp<{wt},false,kModeDelta>",
+                                profile_traffic(kind) if weight == "u32" and method == "delta" else None),
            "phases": st["phases"], "buckets": st["iterations_used"], "delta": st["delta_used"],
            "delta_final": st["delta_final"], "edges_scanned_last": st["edges_scanned"], "clocks": run["clocks"]}
+    if method == "adds":
+        out["work_items_last"] = st["work_items"]
+        out["active_buckets_max_last"] = st["active_buckets_max"]
     if check:
         out["parity"] = parity_check(rp, ci, w if weight == "u32" else np.ascontiguousarray(w, np.float32),
                                      dists, sources[:check], weight)
@@ -541,10 +544,18 @@ def policy_compare(graphs: dict) -> dict:
     try:
         for name, (g, srcs) in graphs.items():
             r = pol.compare(g, srcs[:8], reps=2)
-            r["decision"] = p.decide(pol.graph_features(g))
+            r["network_output"] = p.decide(pol.graph_features(g))
+            if not r["policy_used"]:
+                r["note"] = ("features outside the training graphs' range: the fixed Near-Far schedule runs "
+                             "(the network's output above is not applied)")
             res[name] = r
     finally:
         p.deactivate()
+    w = pol.load_weights()
+    res["training"] = {k: (float(w[k]) if k in w else None) for k in
+                       ("n_graphs", "cv_geo_speedup", "cv_slower_frac", "cv_worst", "cv_oracle_geo_speedup",
+                        "dead_zone")}
+    res["training"]["cv_folds"] = int(w["cv_folds"]) if "cv_folds" in w else None
     return res
 
 
@@ -903,8 +914,8 @@ def workload_policy(args):
         res[name]["learned_gteps"] = reach[name] / res[name]["learned_ms"] / 1e6
         g.close()
     tot_e = sum(reach.values())
-    tot_f = sum(r["fixed_ms"] for r in res.values())
-    tot_l = sum(r["learned_ms"] for r in res.values())
+    tot_f = sum(res[k]["fixed_ms"] for k in graphs)
+    tot_l = sum(res[k]["learned_ms"] for k in graphs)
     return _line("sssp_gteps_learned_schedule", tot_e / tot_l / 1e6, "GTEPS", args, tot_l / 16, "u32",
                  {"workload": f"learned_vs_fixed_delta_rmat{SCALE}_and_grid{GRID_SIDE}_u32", "sources": 8},
                  gpu_launches=32,

@@ -299,6 +299,7 @@ struct b2_graph_s {
   double pol_mult = 1.0;        // active policy's version
   uint32_t pol_fusion = 0;      // bucket-fusion threshold (0: off)
   float pol_pull = 8.0f;        // push/pull switch point (0: push only)
+  bool pol_outside = false;     // the graph's features lie outside the training range: fixed schedule
   b2::Workspace ws;
   std::mutex mu;   // one solve at a time per handle
 };

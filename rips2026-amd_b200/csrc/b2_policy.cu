@@ -225,6 +225,7 @@ constexpr double kLog2MultMin = -4.0, kLog2MultMax = 6.0;   // clamp of output y
 constexpr double kFusionOffBelow = 7.0, kFusionLog2Max = 14.0;   // output y1
 constexpr double kPullOffAbove = 7.0, kPullLog2Min = 0.0;       // output y2
 constexpr int kDepthCap = 256;   // hop-depth probe: at most this many Bellman-Ford rounds
+constexpr float kRangeMargin = 0.1f;   // out-of-range tolerance, as a fraction of each feature's training span
 
 // The 24 features: size (log n, log m, m/n, log max degree), out-degree
 // quantiles of a vertex sample, weight quantiles of an edge sample (relative
@@ -329,6 +330,17 @@ b2_status policy_decide(b2_graph g, double* delta_mult, uint32_t* fusion_thresho
   if (g->pol_version != g_generation) {
     b2_status s = features_cached(g);
     if (s != B2_SUCCESS) return s;
+    // a graph past the training graphs' range (by more than a tenth of the
+    // range in any feature) keeps the fixed schedule: the network was never
+    // shown such a graph and its guess there is not evidence
+    g->pol_outside = false;
+    if (g_active->s.has_range)
+      for (int k = 0; k < kIn; ++k) {
+        const float span = g_active->s.hi[k] - g_active->s.lo[k];
+        const float x = g->features[k];
+        if (x < g_active->s.lo[k] - kRangeMargin * span || x > g_active->s.hi[k] + kRangeMargin * span)
+          g->pol_outside = true;
+      }
     float xn[kIn], y[kOut];
     normalize(g_active, g->features, xn, 1);
     s = run_forward(g_active, xn, 1, y);
@@ -343,6 +355,7 @@ b2_status policy_decide(b2_graph g, double* delta_mult, uint32_t* fusion_thresho
                                                : (float)std::exp2(std::max(kPullLog2Min, (double)y[2]));
     g->pol_version = g_generation;
   }
+  if (g->pol_outside) return B2_NOT_SUPPORTED;   // the caller runs the fixed Near-Far schedule
   *delta_mult = g->pol_mult;
   *fusion_threshold = g->pol_fusion;
   *pull_fraction = g->pol_pull;

@@ -168,27 +168,15 @@ constexpr int kWarpsPerBlock = kThreads / 32;
 constexpr uint32_t kNearBuf = 256, kFarBuf = 256, kSlotBuf = 256, kMemBuf = 128;
 constexpr uint32_t kDenseSpan = 256;   // vertices per sweep work item (8 per lane)
 constexpr uint32_t kListBuf = kDenseSpan + 32;   // one span's vertices + fewer than 32 carried
-// Deferred label atomics: a relaxation whose candidate beats the label it
-// read is parked (target, label word) in the warp's pending list; the atomics
-// and the routing run 32 at a time, one per lane.  Only a few per cent of the
-// relaxed edges improve a label, yet nearly every 128-edge step holds one,
-// so issuing atomics per step would add two dependent L2 round trips (label
-// atomic, dedup stamp) to almost every step.
-constexpr uint32_t kPend = 64;
-constexpr uint32_t kPendOff = kNearBuf + kFarBuf + 2 * kSlotBuf + kMemBuf + kListBuf;   // even: 8-byte aligned
-constexpr uint32_t kStageWords = kPendOff + 3 * kPend;   // + label words (2 words each) + targets
+constexpr uint32_t kStageWords = kNearBuf + kFarBuf + 2 * kSlotBuf + kMemBuf + kListBuf;
 constexpr size_t kStageBytes = (size_t)kWarpsPerBlock * kStageWords * 4;
-static_assert(kPendOff % 2 == 0 && kStageWords % 2 == 0, "pending label words need 8-byte alignment");
 struct WarpQ {
-  uint32_t* nearb;   // kNearBuf vertex ids (the start of the warp's staging area)
+  uint32_t* nearb;   // kNearBuf vertex ids
   uint32_t* farb;    // kFarBuf
   uint32_t* slotb;   // kSlotBuf (vertex, slot) pairs as 2 words
   uint32_t* memb;    // kMemBuf
   uint32_t* listb;   // kListBuf frontier vertices found by a sweep
-  uint32_t nn = 0, nf = 0, ns = 0, nm = 0, np = 0;
-  template <class T>
-  __device__ __forceinline__ T* pend_w() const { return reinterpret_cast<T*>(nearb + kPendOff); }
-  __device__ __forceinline__ uint32_t* pend_v() const { return nearb + kPendOff + 2 * kPend; }
+  uint32_t nn = 0, nf = 0, ns = 0, nm = 0;
 };
 
 struct Tally {
@@ -426,43 +414,8 @@ __device__ __forceinline__ void route_batch(const Params& P, const PhaseRec& R, 
   }
 }
 
-// Issue the label atomics of the last 32 (or, with `all`, every remaining
-// fewer) pending relaxations, one per lane, and route the improvements
-// (warp-collective).
-template <class W, bool PRED, int MODE>
-__device__ __forceinline__ void drain_pending(const Params& P, const PhaseRec& R, Tally& t, bool all) {
-  using L = Label<PRED>;
-  while (t.q.np >= 32 || (all && t.q.np > 0)) {
-    const uint32_t k = min(t.q.np, 32u);
-    const uint32_t i = t.q.np - k + lane_id();
-    const bool has = lane_id() < k;
-    __syncwarp();   // the appends of other lanes are visible
-    uint2 ed[1];
-    uint32_t cand[1];
-    bool imp[1];
-    typename L::T cw = L::kInf;
-    ed[0] = make_uint2(0u, 0u);
-    if (has) {
-      ed[0].x = t.q.pend_v()[i];
-      cw = t.q.template pend_w<typename L::T>()[i];
-    }
-    __syncwarp();   // every lane has read its entry before the list is appended to again
-    t.q.np -= k;
-    cand[0] = has ? L::key(cw) : kInfKey;
-    const typename L::T old =
-        atom_min_keep_if(has, (typename L::T*)P.dist + ed[0].x, cw, t.keep, (typename L::T)0);
-    // (PRED: a smaller predecessor at an equal distance updates the word
-    //  but does not re-expand the vertex.)
-    imp[0] = cand[0] < L::key(old);
-    t.impr += imp[0] ? 1 : 0;
-    route_batch<W, MODE, 1>(P, R, imp, ed, cand, t);
-    flush_all<MODE>(P, R, t.q, false);
-  }
-}
-
-// Relax U edge slots per lane: the label loads of every slot, then the
-// candidates that beat the label read are parked in the warp's pending list
-// (drained 32 at a time).
+// Relax U edge slots per lane: label loads first, then the atomics of every
+// slot (issued before any result is read), then routing.
 template <class W, bool PRED, int MODE, int U>
 __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, const bool (&act)[U],
                                             const uint32_t (&src)[U], const uint32_t (&dsrc)[U],
@@ -470,7 +423,8 @@ __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, 
   using L = Label<PRED>;
   typename L::T* lab = (typename L::T*)P.dist;
   uint32_t cand[U];
-  typename L::T cur[U];
+  typename L::T cur[U], old[U];
+  bool imp[U];
 #pragma unroll
   for (int q = 0; q < U; ++q) {
     cand[q] = act[q] ? W::extend(dsrc[q], ed[q].y) : kInfKey;
@@ -479,17 +433,18 @@ __device__ __forceinline__ void relax_batch(const Params& P, const PhaseRec& R, 
 #pragma unroll
   for (int q = 0; q < U; ++q) {
     const typename L::T cw = L::make(cand[q], src[q]);
-    const bool want = cand[q] != kInfKey && cw < cur[q];
-    const uint32_t bal = __ballot_sync(0xffffffffu, want);
-    if (want) {
-      const uint32_t i = t.q.np + __popc(bal & ((1u << lane_id()) - 1u));
-      t.q.pend_v()[i] = ed[q].x;
-      t.q.template pend_w<typename L::T>()[i] = cw;
-    }
-    t.q.np += __popc(bal);
-    t.edges += act[q] ? 1 : 0;
-    if (t.q.np >= 32) drain_pending<W, PRED, MODE>(P, R, t, false);   // keeps np < 32 + 32 <= kPend
+    // not issued: old = 0 reads as "no improvement"
+    old[q] = atom_min_keep_if(cand[q] != kInfKey && cw < cur[q], lab + ed[q].x, cw, t.keep, (typename L::T)0);
   }
+#pragma unroll
+  for (int q = 0; q < U; ++q) {
+    // (PRED: a smaller predecessor at an equal distance updates the word
+    //  but does not re-expand the vertex.)
+    imp[q] = cand[q] < L::key(old[q]);
+    t.edges += act[q] ? 1 : 0;
+    t.impr += imp[q] ? 1 : 0;
+  }
+  route_batch<W, MODE, U>(P, R, imp, ed, cand, t);
 }
 
 template <class W, bool PRED, int MODE>
@@ -518,51 +473,37 @@ __device__ __forceinline__ void phase_range(const Params& P, const PhaseRec& R, 
 }
 
 // ---------------------------------------------------------------------------
-// Hub chunks [first, first + cnt) (cnt <= 32): 256 consecutive edges each of a
-// high-degree vertex's phase range.  Lane i loads chunk i's entry, row bounds
-// and source label, so the setup of every chunk of the work item costs two
-// memory round trips in all; then the warp walks the chunks' edges in turn.
+// One hub chunk: 256 consecutive edges of a high-degree vertex's phase range.
 template <class W, bool PRED, int MODE>
-__device__ __forceinline__ void hub_chunks(const Params& P, const PhaseRec& R, uint32_t first, uint32_t cnt,
-                                           Tally& t) {
+__device__ __forceinline__ void hub_chunk(const Params& P, const PhaseRec& R, uint32_t item, Tally& t) {
   const uint32_t lane = lane_id();
   const HubEntry* H = P.hubs + (size_t)(R.hub_in & 1) * P.hub_cap;
-  uint32_t hv = 0, du = kInfKey;
-  uint64_t e0 = 0, e1 = 0;
-  if (lane < cnt) {
-    const uint2 h = ldcg(reinterpret_cast<const uint2*>(H + first + lane));
-    hv = h.x;
-    uint64_t rlo, rhi;
-    bool hh;
-    phase_range(P, R, hv, rlo, rhi, hh);   // issued with the label load
-    du = src_key<W, PRED, MODE>(P, hv);
-    bool valid = du != kInfKey;
-    if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
-    if (valid) {
-      e0 = rlo + (uint64_t)h.y * kHubChunk;
-      e1 = min(rhi, e0 + kHubChunk);
-    }
-  }
+  const uint2 h = ldcg(reinterpret_cast<const uint2*>(H + item));
+  const uint32_t v = h.x;
+  uint64_t rlo, rhi;
+  bool hh;
+  phase_range(P, R, v, rlo, rhi, hh);   // issued with the label load
+  const uint32_t du = src_key<W, PRED, MODE>(P, v);
+  bool valid = du != kInfKey;
+  if (MODE == kModeDelta) valid = valid && bucket_of<W>(R, du) == R.cur;
+  if (!valid) return;
+  const uint64_t e0 = rlo + (uint64_t)h.y * kHubChunk;
+  const uint64_t e1 = min(rhi, e0 + kHubChunk);
   // B2_HUB_UNROLL edge loads per lane in flight per step
   constexpr int U = B2_HUB_UNROLL;
-  for (uint32_t c = 0; c < cnt; ++c) {
-    const uint32_t v = __shfl_sync(0xffffffffu, hv, c);
-    const uint32_t dv = __shfl_sync(0xffffffffu, du, c);
-    const uint64_t c0 = shfl64(e0, c), c1 = shfl64(e1, c);
-    for (uint64_t eb = c0; eb < c1; eb += 32 * U) {
-      bool act[U];
-      uint32_t src[U], dsrc[U];
-      uint2 ed[U];
+  for (uint64_t eb = e0; eb < e1; eb += 32 * U) {
+    bool act[U];
+    uint32_t src[U], dsrc[U];
+    uint2 ed[U];
 #pragma unroll
-      for (int q = 0; q < U; ++q) {
-        const uint64_t e = eb + 32 * q + lane;
-        act[q] = e < c1;
-        src[q] = v;
-        dsrc[q] = dv;
-        ed[q] = act[q] ? __ldcs(&P.edges[e]) : make_uint2(0, 0);
-      }
-      relax_batch<W, PRED, MODE, U>(P, R, act, src, dsrc, ed, t);
+    for (int q = 0; q < U; ++q) {
+      const uint64_t e = eb + 32 * q + lane;
+      act[q] = e < e1;
+      src[q] = v;
+      dsrc[q] = du;
+      ed[q] = act[q] ? __ldcs(&P.edges[e]) : make_uint2(0, 0);
     }
+    relax_batch<W, PRED, MODE, U>(P, R, act, src, dsrc, ed, t);
   }
 }
 
@@ -588,39 +529,32 @@ __device__ __forceinline__ void expand_vertices(const Params& P, const PhaseRec&
       has_heavy = false;
     }
   }
-  // settled in this light round: its heavy suffix is relaxed once by the
-  // heavy phase.  The dedup exchange goes out now and is read after the
-  // edges below are relaxed, so it adds no round trip of its own.
-  uint32_t hold = R.hround;
-  const uint32_t hcount = (uint32_t)min(row_end - hi, (uint64_t)0xFFFFFFFFull);
   if (MODE == kModeDelta) {
     if (__any_sync(0xffffffffu, valid) && lane == 0 && ldcg(&c->bucket_valid) == 0) c->bucket_valid = 1;
     if (members) {
-      hold = atom_exch_if(valid && has_heavy, &P.hstamp[v], R.hround, R.hround);
+      // settled in this light round: its heavy suffix is relaxed once by the heavy phase
+      const bool want = valid && has_heavy && atomicExch(&P.hstamp[v], R.hround) != R.hround;
       if (P.in_rowptr) {
-        // the bucket's smallest label (the pull's early-exit bound)
+        // push cost of the heavy pass and the bucket's smallest label (the pull's early-exit bound)
+        unsigned long long hv = want ? (unsigned long long)(row_end - hi) : 0ull;
         uint32_t mk = valid ? du : 0xFFFFFFFFu;
-        mk = __reduce_min_sync(0xffffffffu, mk);
-        if (lane == 0 && mk != 0xFFFFFFFFu) atomicMin(&c->cur_min_key, mk);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          hv += __shfl_xor_sync(0xffffffffu, hv, o);
+          mk = min(mk, __shfl_xor_sync(0xffffffffu, mk, o));
+        }
+        if (lane == 0) {
+          if (hv) atomicAdd(&c->member_heavy, hv);
+          if (mk != 0xFFFFFFFFu) atomicMin(&c->cur_min_key, mk);
+        }
+      }
+      stage(t.q.memb, t.q.nm, want, v);
+      if (t.q.nm > kMemBuf / 2) {
+        publish(P, &c->members_count, kQMembers, t.q.memb, t.q.nm, 14);
+        t.q.nm = 0;
       }
     }
   }
-  const auto stage_members = [&]() {
-    if (MODE != kModeDelta || !members) return;
-    const bool want = valid && has_heavy && hold != R.hround;
-    if (P.in_rowptr) {
-      // push cost of the heavy pass
-      unsigned long long hv = want ? (unsigned long long)hcount : 0ull;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) hv += __shfl_xor_sync(0xffffffffu, hv, o);
-      if (lane == 0 && hv) atomicAdd(&c->member_heavy, hv);
-    }
-    stage(t.q.memb, t.q.nm, want, v);
-    if (t.q.nm > kMemBuf / 2) {
-      publish(P, &c->members_count, kQMembers, t.q.memb, t.q.nm, 14);
-      t.q.nm = 0;
-    }
-  };
   uint32_t deg = valid ? (uint32_t)min(hi - lo, (uint64_t)0xFFFFFFFFull) : 0u;
   // high-degree ranges -> one hub-list entry per 256-edge chunk, written by
   // the whole warp, taken by any warp in the next phase
@@ -646,10 +580,7 @@ __device__ __forceinline__ void expand_vertices(const Params& P, const PhaseRec&
   // compact the lanes that have edges to relax
   const uint32_t nz = __ballot_sync(0xffffffffu, deg > 0);
   const uint32_t k = __popc(nz);
-  if (k == 0) {
-    stage_members();
-    return;
-  }
+  if (k == 0) return;
   const bool has = lane < k;
   const uint32_t sl = nth_set_bit(nz, has ? lane : 0u);
   const uint32_t cv = __shfl_sync(0xffffffffu, v, sl);
@@ -683,7 +614,6 @@ __device__ __forceinline__ void expand_vertices(const Params& P, const PhaseRec&
     }
     relax_batch<W, PRED, MODE, kUnroll>(P, R, act, src, dsrc, ed, t);
   }
-  stage_members();
 }
 
 // Append the frontier's vertices among [span * 256, span * 256 + 256) (stamp
@@ -767,7 +697,6 @@ __device__ __forceinline__ void frontier_chunk(const Params& P, const PhaseRec& 
 }
 
 constexpr uint32_t kHubGrab = B2_HUB_GRAB;   // hub chunks per work item
-static_assert(kHubGrab >= 1 && kHubGrab <= 32, "a hub work item's chunks are set up one per lane");
 
 // A relaxation phase: hub chunks of the previous phase, then 32-vertex
 // frontier chunks (or 256-vertex sweep items).  Items are first dealt
@@ -807,14 +736,13 @@ __device__ void process_phase(const Params& P, const PhaseRec& R, Tally& t) {
     const bool done = item >= items;
     if (done && carry == 0) break;
     if (!done && item < nhg) {
-      const uint32_t h0 = item * kHubGrab;
-      hub_chunks<W, PRED, MODE>(P, R, h0, min(nhub, h0 + kHubGrab) - h0, t);
+      const uint32_t h1 = min(nhub, (item + 1) * kHubGrab);
+      for (uint32_t h = item * kHubGrab; h < h1; ++h) hub_chunk<W, PRED, MODE>(P, R, h, t);
     } else {
       frontier_item<W, PRED, MODE>(P, R, done ? 0u : item - nhg, dense, done, carry, t, g);
     }
     if (done) break;
   }
-  drain_pending<W, PRED, MODE>(P, R, t, true);
   flush_all<MODE>(P, R, t.q, true);
 }
 
@@ -1275,7 +1203,6 @@ __device__ void local_phase(const Params& P, const PhaseRec& R0, Tally& t) {
     const unsigned long long e0 = t.edges;
     const uint32_t nfc = (L.fcount + 31) / 32;
     for (uint32_t ch = w; ch < nfc; ch += nw) frontier_chunk<W, PRED, MODE>(P, L, ch * 32, t);
-    drain_pending<W, PRED, MODE>(P, L, t, true);
     flush_all<MODE>(P, L, t.q, true);
     {
       unsigned long long de = t.edges - e0;
@@ -1319,7 +1246,7 @@ template <class W, bool PRED, int MODE>
 __global__ void __launch_bounds__(kThreads, B2_SSSP_MINB) k_sssp(Params P) {
   using L = Label<PRED>;
   __shared__ PhaseRec s_rec;
-  extern __shared__ __align__(16) uint32_t s_stage[];   // kStageWords per warp
+  extern __shared__ uint32_t s_stage[];   // kStageWords per warp
   Tally t;
   t.keep = l2_keep_policy();
   {
