@@ -138,18 +138,24 @@ def test_features_are_cached_and_sane(pol, b2, cuda):
 
 
 def test_shipped_policy_keeps_distances(pol, b2, orc, cuda):
+    """The shipped weights pick the schedule of graphs inside their training
+    range (2^14 - 2^22 vertices) and leave graphs outside it on the fixed
+    Near-Far schedule; distances and predecessor trees are exact either way."""
     p = pol.activate_default()
-    for hg, weight, s in [(b2.gen_rmat(15, 16, seed=9), "u32", 1), (b2.gen_grid(90, 70, 0.02, seed=3), "f32", 5),
-                          (b2.gen_er(5000, 40000, 1, 1000, seed=1), "u32", 0)]:
+    for hg, weight, s, inside in [(b2.gen_rmat(15, 16, seed=9), "u32", 1, True),
+                                  (b2.gen_grid(150, 140, 0.02, seed=3), "f32", 5, True),
+                                  (b2.gen_er(20000, 160000, 1, 1000, seed=1), "u32", 0, True),
+                                  (b2.gen_er(2000, 16000, 1, 1000, seed=2), "u32", 0, False)]:
         g = b2.Graph.from_host(hg, weight)
         w = hg.weights if weight == "u32" else hg.fweights
         ref = orc.dijkstra(hg.rowptr, hg.colind, w, s)
         for method in ("delta", "adds"):
             d, pr, st = g.sssp(s, method=method, policy=1, pred=True)
-            assert st["policy_used"] == 1
+            assert st["policy_used"] == (1 if inside else 0), (hg.n, method)
             got = _raw(d, weight)
             assert np.array_equal(got, ref)
             assert orc.validate_spt(hg.rowptr, hg.colind, w, s, got, pr.cpu().numpy()) == 0
+        g.close()
     p.deactivate()
 
 
